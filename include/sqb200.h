@@ -1,0 +1,85 @@
+/*
+ * sqb200.h -- C ABI of the B200 two-electron Fock build (Coulomb J and exchange K).
+ *
+ * Plain C types only: every entry point returns an int status (0 = success, negative =
+ * error, see SQB200_E*), never exits, and keeps the last error text for sqb200_last_error().
+ *
+ * Basis functions are described exactly as the reference's struct GTOBasis_t
+ * (src/basis.h:21-32) in genBasis order (src/basis.c:529-623), flattened:
+ *   nprim[i]             nContract of function i
+ *   lmn[3i..3i+2]        angular indices l, m, n
+ *   xyz[3i..3i+2]        centre (bohr)
+ *   exps[], ncoefs[]     primitives of all functions concatenated in function order;
+ *                        ncoefs = norm[k]*coef[k] (the weight genGTOShell stores,
+ *                        src/matrix.c:2510-2512)
+ * Density and output matrices are nbf x nbf row-major float64.
+ */
+#ifndef SQB200_H
+#define SQB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SQB200_OK            0
+#define SQB200_EINVAL       -1   /* bad argument                                  */
+#define SQB200_EUNSUPPORTED -2   /* shell type beyond d, or non-canonical order   */
+#define SQB200_ENOMEM       -3   /* device or host allocation failed              */
+#define SQB200_ECUDA        -4   /* CUDA runtime error                            */
+#define SQB200_ENODEV       -5   /* no usable CUDA device                         */
+
+typedef struct sqb200_jk sqb200_jk;   /* opaque per-basis device context */
+
+/* Create a context: shells and shell-pair Hermite data resident on `device`.
+ * Replaces the first-visit set-up of GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3830-3886:
+ * genGTOShell, sortGTOShell, shell-level Schwarz).  `schwarz` is the basis-level Schwarz
+ * matrix of create_Schwarz (src/matrix.c:389) the caller already holds (the argument
+ * `Schwarz` of uhf_getGMatrix, src/uhf.c:112); pass NULL to compute it on the device. */
+int sqb200_jk_create(sqb200_jk **ctx, int nbf, const int *nprim, const int *lmn,
+                     const double *xyz, const double *exps, const double *ncoefs,
+                     const double *schwarz, int device);
+
+/* Release everything the context holds (the reset call nBasis==0 of
+ * GTO_JK_Matrix_Quartet_Parallel, src/matrix.c:3818-3828). */
+int sqb200_jk_destroy(sqb200_jk *ctx);
+
+/* One J/K build from host densities into host outputs, overwriting JT, KA, KB.
+ * Semantics of GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3773-3986) for one process:
+ *   JT = J[PA+PB];  KA = -K[PA];  KB = -K[PB] (KB = KA when restricted);  all symmetric.
+ * A shell quartet is skipped when r = Sch(PQ)*Sch(IJ) < scf_cutoff or r < fixed_cutoff
+ * (src/matrix.c:3914-3919), and, for r < dscreen_rmax, when r * maxPShell < fixed_cutoff
+ * (src/matrix.c:3921-3943).  A primitive quartet is skipped when its prefactor is below
+ * 1e-15 (src/int.c:1282).  PB may equal PA.  Synchronous. */
+int sqb200_jk_build(sqb200_jk *ctx, const double *PA, const double *PB, int restricted,
+                    double scf_cutoff, double fixed_cutoff, double dscreen_rmax,
+                    double *JT, double *KA, double *KB);
+
+/* The same build on device buffers (allocated on the context's device) enqueued on
+ * `stream` (a cudaStream_t, or NULL for the context's own stream).  Does not synchronise.
+ * dPB may equal dPA; dKB may be NULL when restricted. */
+int sqb200_jk_build_device(sqb200_jk *ctx, const double *dPA, const double *dPB,
+                           int restricted, double scf_cutoff, double fixed_cutoff,
+                           double dscreen_rmax, double *dJT, double *dKA, double *dKB,
+                           void *stream);
+
+/* Counters of the last build: out[0] shell quartets computed, out[1] primitive quartets
+ * evaluated, out[2] algorithmic FP64 operations (per-class operation table),
+ * out[3] shells, out[4] shell pairs.  Synchronises the context stream. */
+int sqb200_jk_stats(sqb200_jk *ctx, long long *out, int n);
+
+/* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,
+ * src/matrix.c:389-440), written to the host array S (nbf*nbf). */
+int sqb200_jk_schwarz(sqb200_jk *ctx, double *S);
+
+/* Memory cutoff of getMemCutoff_Parallel (src/matrix.c:3703-3760) for nCPU=1 and maxMem
+ * in MB: the Schwarz product above which the reference's first visit skips the density
+ * screen (pass it as dscreen_rmax to reproduce a first reference visit). */
+int sqb200_jk_mem_cutoff(sqb200_jk *ctx, double fixed_cutoff, int max_mem_mb, double *out);
+
+/* Text of the last error on this thread. */
+const char *sqb200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

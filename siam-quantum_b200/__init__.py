@@ -1,0 +1,13 @@
+"""siam-quantum_b200: B200-native two-electron Fock build (J/K) for Siam Quantum 2.
+
+The product is the CUDA library libsqb200.so behind the C ABI in include/sqb200.h.  This
+Python package is the host-side binding used by tests and the benchmark:
+  engine     ctypes binding of the C ABI (JKEngine)
+  basis      genBasis-order Cartesian Gaussian basis builder (flat arrays for the ABI)
+  molecules  seeded workload geometries (water, benzene, C60, random organics)
+
+The directory name is not a Python identifier; import it with `load_package()` from a
+checkout root or via importlib (see tests/conftest.py).
+"""
+from . import basis, engine, molecules  # noqa: F401
+from .engine import JKEngine, SQB200Error, load_library  # noqa: F401

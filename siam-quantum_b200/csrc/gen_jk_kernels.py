@@ -1,0 +1,394 @@
+"""Generate the per-class J/K CUDA kernels (McMurchie-Davidson ERI + fused digestion).
+
+One kernel per quartet class (bra pair class | ket pair class) and spin mode (R: restricted,
+K from PA only; U: unrestricted, K from PA and PB).  A CTA owns one bra shell pair and up to
+128 ket shell pairs (one shell quartet per thread).  For each quartet the thread evaluates
+
+    (ab|cd) = sum_{bra prims i} sum_{tuv} Eb_i[ab][tuv] *
+              sum_{ket prims j} sum_{tau nu phi} (-1)^(tau+nu+phi) Ek_j[cd][tau nu phi] R_ij[t+tau, u+nu, v+phi]
+
+where Eb/Ek are Hermite expansion coefficients (with contraction coefficients, exp(-mu R^2)/p
+and 1/q folded in, precomputed per primitive pair on the host) and R are the Hermite Coulomb
+integrals built from the Boys function.  The inner sum over ket primitives is accumulated in
+Hermite space (G[cd][tuv]); the bra transform runs once per bra primitive.  When the per-thread
+state would not fit in registers the ket functions are processed in blocks ("passes"), each
+pass repeating the primitive loop.  The contracted block is digested at once into
+
+    Jacc[ab] += 2 deg PT[cd] v     Jacc[cd] += 2 deg PT[ab] v
+    Kacc[ac] += deg P[bd] v        Kacc[bc] += deg P[ad] v
+    Kacc[ad] += deg P[bc] v        Kacc[bd] += deg P[ac] v
+
+(deg = 1/2 per coinciding bra shells, ket shells and bra==ket pair), so J = Jacc + Jacc^T and
+K = Kacc + Kacc^T.  This reproduces what the reference's storeQuartetEE (src/matrix.c:2934)
+accumulates for the six degeneracy cases.
+
+The generator also counts the floating-point operations it emits per primitive quartet, per
+bra-primitive flush and per quartet (FMA = 2) and writes that table (jk_flops.json) as the
+algorithmic work W(class) used for roofline reporting.
+
+Usage: python gen_jk_kernels.py <outdir>
+"""
+import itertools
+import json
+import os
+import sys
+
+COMP = {
+    "S": [(0, 0, 0)],
+    "L": [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)],
+    "P": [(1, 0, 0), (0, 1, 0), (0, 0, 1)],
+    "D": [(2, 0, 0), (0, 2, 0), (0, 0, 2), (1, 1, 0), (1, 0, 1), (0, 1, 1)],
+}
+LMAX = {"S": 0, "L": 1, "P": 1, "D": 2}
+TYPE_ID = {"S": 0, "L": 1, "P": 2, "D": 3}        # reference sort order (src/matrix.h:238-244)
+# pair classes (type of the first shell >= type of the second in the reference order)
+PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
+# bra/ket orientation: the larger pair (by functions, then L) is the bra
+PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
+STATE_MAX = 64          # doubles of G + out accumulators per pass
+CTA = 128
+
+
+def pair_funcs(pc):
+    a, b = pc
+    return [(ca, cb) for ca in COMP[a] for cb in COMP[b]]
+
+
+def nz(f):
+    (ax, ay, az), (bx, by, bz) = f
+    return [(t, u, v) for t in range(ax + bx + 1) for u in range(ay + by + 1) for v in range(az + bz + 1)]
+
+
+def etable(pc):
+    """E-table layout: list of (function index, (t,u,v)) in storage order, and offsets."""
+    fs = pair_funcs(pc)
+    off, lay = [], []
+    for fi, f in enumerate(fs):
+        off.append(len(lay))
+        for h in nz(f):
+            lay.append((fi, h))
+    return fs, off, lay
+
+
+def pair_L(pc):
+    return LMAX[pc[0]] + LMAX[pc[1]]
+
+
+class Emitter:
+    def __init__(self):
+        self.lines = []
+        self.ind = 1
+
+    def __call__(self, s):
+        self.lines.append("  " * self.ind + s)
+
+
+def gen_R(em, L, need):
+    """Emit R^{(0)}_{tuv} for (t,u,v) in need; returns flop count and name map."""
+    have = {}
+    flops = [0]
+
+    def get(n, t, u, v):
+        key = (n, t, u, v)
+        if key in have:
+            return have[key]
+        if t == 0 and u == 0 and v == 0:
+            have[key] = "b%d" % n
+            return have[key]
+        name = "r%d_%d_%d_%d" % key
+        if t > 0:
+            d, ax, lo = t, "X", (n + 1, t - 2, u, v)
+            hi = (n + 1, t - 1, u, v)
+        elif u > 0:
+            d, ax, lo = u, "Y", (n + 1, t, u - 2, v)
+            hi = (n + 1, t, u - 1, v)
+        else:
+            d, ax, lo = v, "Z", (n + 1, t, u, v - 2)
+            hi = (n + 1, t, u, v - 1)
+        h = get(*hi)
+        if d - 1 > 0:
+            l_ = get(*lo)
+            if d - 1 == 1:
+                em("const double %s = fma(%s, %s, %s);" % (name, ax, h, l_))
+                flops[0] += 2
+            else:
+                em("const double %s = fma(%s, %s, %d.0 * %s);" % (name, ax, h, d - 1, l_))
+                flops[0] += 3
+        else:
+            em("const double %s = %s * %s;" % (name, ax, h))
+            flops[0] += 1
+        have[key] = name
+        return name
+
+    names = {}
+    for (t, u, v) in sorted(need, key=lambda x: (sum(x), x)):
+        names[(t, u, v)] = get(0, t, u, v)
+    return names, flops[0]
+
+
+def boys_flops(M):
+    # Taylor Horner (9 terms: 8 fma + 8 mul), downward recursion (fma + mul per order),
+    # argument setup not counted here
+    return 8 * 3 + M * 3
+
+
+def gen_class(bra, ket, spin):
+    """Return (kernel source, metadata) for class (bra|ket) and spin 'R' or 'U'."""
+    fb, offb, layb = etable(bra)
+    fk, offk, layk = etable(ket)
+    nab, ncd = len(fb), len(fk)
+    Lb, Lk = pair_L(bra), pair_L(ket)
+    Lt = Lb + Lk
+    Hb = sorted({h for f in fb for h in nz(f)}, key=lambda x: (sum(x), x))
+    hidx = {h: i for i, h in enumerate(Hb)}
+    na, nb_ = len(COMP[bra[0]]), len(COMP[bra[1]])
+    nc, nd = len(COMP[ket[0]]), len(COMP[ket[1]])
+    NB = 5 + len(layb)
+    NK = 5 + len(layk)
+    per = max(1, STATE_MAX // (len(Hb) + nab))
+    blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
+    name = "jk_%s_%s_%s" % (bra, ket, spin)
+    fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks)}
+
+    em = Emitter()
+    out = []
+    out.append('extern "C" __global__ void __launch_bounds__(%d)' % CTA)
+    out.append("%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name)
+    em("extern __shared__ double sbra[];")
+    em("const sqb::WorkItem it = items[blockIdx.x];")
+    em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
+    em("const int N = a.nbf;")
+    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
+    em("__syncthreads();")
+    em("const int tid = threadIdx.x;")
+    em("bool ok = tid < it.cnt;")
+    em("sqb::PairRec kp = bp;")
+    em("double deg = 0.0;")
+    em("if (ok) {")
+    em.ind += 1
+    em("kp = a.ket_pairs[it.k0 + tid];")
+    em("const double r = bp.schwarz * kp.schwarz;")
+    em("ok = !(r < a.cut_outer) && !(r < a.cut_fixed);")
+    em("if (ok && r < a.dscreen_rmax) {")
+    em("  const bool bf = (bp.P > kp.P) || (bp.P == kp.P && bp.Q >= kp.Q);")
+    em("  const int P = bf ? bp.P : kp.P, Q = bf ? bp.Q : kp.Q, I = bf ? kp.P : bp.P, J = bf ? kp.Q : bp.Q;")
+    em("  const double* PM = a.PM; const int ns = a.ns;")
+    em("  const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];")
+    em("  ok = !(r * mp < a.cut_fixed);")
+    em("}")
+    em("deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + tid) ? 0.5 : 1.0);")
+    em.ind -= 1
+    em("}")
+    for ab in range(nab):
+        em("double jab%d = 0.0;" % ab)
+    em("unsigned long long nprimq = 0, nflush = 0;")
+    em("if (ok) {")
+    em.ind += 1
+    em("const double* __restrict__ kprim = a.ket_prims + kp.poff;")
+    em("const int nbp = bp.nprim, nkp = kp.nprim;")
+    em("nflush = nbp;")
+    em("const double* __restrict__ PA = a.PA;")
+    if spin == "U":
+        em("const double* __restrict__ PB = a.PB;")
+    em("const double* __restrict__ PT = a.PT;")
+    for bi, blk in enumerate(blocks):
+        em("{  // pass %d: ket functions %s" % (bi, blk))
+        em.ind += 1
+        for ab in range(nab):
+            for cd in blk:
+                em("double o%d_%d = 0.0;" % (ab, cd))
+        em("for (int i = 0; i < nbp; ++i) {")
+        em.ind += 1
+        em("const double* __restrict__ bi = sbra + i * %d;" % NB)
+        em("const double p = bi[0], Px = bi[1], Py = bi[2], Pz = bi[3], kpb = bi[4];")
+        for cd in blk:
+            for h in Hb:
+                em("double g%d_%d = 0.0;" % (cd, hidx[h]))
+        em("for (int j = 0; j < nkp; ++j) {")
+        em.ind += 1
+        em("const double* __restrict__ kj = kprim + j * %d;" % NK)
+        em("const double q = kj[0];")
+        em("const double pq = p + q;")
+        em("const double rs = rsqrt(pq);")
+        em("if (TWO_PI_2_5 * kpb * kj[4] * rs < PRIM_CUTOFF) continue;")
+        if bi == 0:
+            em("++nprimq;")
+        em("const double alpha = p * q * (rs * rs);")
+        em("const double X = Px - kj[1], Y = Py - kj[2], Z = Pz - kj[3];")
+        em("const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));")
+        em("double F[%d];" % (Lt + 1))
+        em("sqb::boys<%d>(T, a.boys_tab, F);" % Lt)
+        em("const double s0 = TWO_PI_2_5 * rs;")
+        em("const double m2a = -2.0 * alpha;")
+        em("double w = s0;")
+        pf = 9 + 2 + 3 + 5 + boys_flops(Lt) + 2  # setup: pq, alpha, XYZ diff, T, s0, m2a
+        for n in range(Lt + 1):
+            if n > 0:
+                em("w *= m2a;")
+                pf += 1
+            em("const double b%d = w * F[%d];" % (n, n))
+            pf += 1
+        need = set()
+        for cd in blk:
+            for (tau, nu, phi) in nz(fk[cd]):
+                for h in Hb:
+                    need.add((h[0] + tau, h[1] + nu, h[2] + phi))
+        rn, rf = gen_R(em, Lt, need)
+        pf += rf
+        for cd in blk:
+            for k, (tau, nu, phi) in enumerate(nz(fk[cd])):
+                e = offk[cd] + k
+                sign = -1 if (tau + nu + phi) % 2 else 1
+                em("{ const double ek = %skj[%d];" % ("-" if sign < 0 else "", 5 + e))
+                for h in Hb:
+                    rr = rn[(h[0] + tau, h[1] + nu, h[2] + phi)]
+                    em("  g%d_%d = fma(ek, %s, g%d_%d);" % (cd, hidx[h], rr, cd, hidx[h]))
+                    pf += 2
+                em("}")
+        em.ind -= 1
+        em("}")
+        # flush: o[ab][cd] += sum_h Eb[ab][h] g[cd][h]
+        ff = 0
+        for ab in range(nab):
+            for k, h in enumerate(nz(fb[ab])):
+                e = offb[ab] + k
+                em("{ const double eb = bi[%d];" % (5 + e))
+                for cd in blk:
+                    em("  o%d_%d = fma(eb, g%d_%d, o%d_%d);" % (ab, cd, cd, hidx[h], ab, cd))
+                    ff += 2
+                em("}")
+        em.ind -= 1
+        em("}")
+        fl["prim"] += pf
+        fl["flush"] += ff
+        # digestion of this block
+        qf = 0
+        cset = sorted({cd // nd for cd in blk})
+        dset = sorted({cd % nd for cd in blk})
+        em("{  // digest")
+        em.ind += 1
+        em("const int fP = bp.fP, fQ = bp.fQ, fI = kp.fP, fJ = kp.fQ;")
+        # densities needed
+        for cd in blk:
+            c, d = divmod(cd, nd)
+            em("const double ptk%d = PT[(fI + %d) * N + fJ + %d];" % (cd, c, d))
+        for ab in range(nab):
+            aa, bb = divmod(ab, nb_)
+            em("const double ptb%d = PT[(fP + %d) * N + fQ + %d];" % (ab, aa, bb))
+        spins = [("A", "PA")] + ([("B", "PB")] if spin == "U" else [])
+        for s, P_ in spins:
+            for bb in range(nb_):
+                for d in dset:
+                    em("const double %sbd%d_%d = %s[(fQ + %d) * N + fJ + %d];" % (s, bb, d, P_, bb, d))
+            for aa in range(na):
+                for d in dset:
+                    em("const double %sad%d_%d = %s[(fP + %d) * N + fJ + %d];" % (s, aa, d, P_, aa, d))
+            for bb in range(nb_):
+                for c in cset:
+                    em("const double %sbc%d_%d = %s[(fQ + %d) * N + fI + %d];" % (s, bb, c, P_, bb, c))
+            for aa in range(na):
+                for c in cset:
+                    em("const double %sac%d_%d = %s[(fP + %d) * N + fI + %d];" % (s, aa, c, P_, aa, c))
+        # J
+        for ab in range(nab):
+            terms = " + ".join("o%d_%d * ptk%d" % (ab, cd, cd) for cd in blk)
+            em("jab%d += %s;" % (ab, terms))
+            qf += 2 * len(blk)
+        for cd in blk:
+            c, d = divmod(cd, nd)
+            terms = " + ".join("o%d_%d * ptb%d" % (ab, cd, ab) for ab in range(nab))
+            em("atomicAdd(a.Jacc + (fI + %d) * N + fJ + %d, 2.0 * deg * (%s));" % (c, d, terms))
+            qf += 2 * nab + 2
+        # K
+        for s, _ in spins:
+            acc = "a.KAacc" if s == "A" else "a.KBacc"
+            tg = {}
+            for ab in range(nab):
+                aa, bb = divmod(ab, nb_)
+                for cd in blk:
+                    c, d = divmod(cd, nd)
+                    o = "o%d_%d" % (ab, cd)
+                    tg.setdefault(("P", aa, "I", c), []).append("%s * %sbd%d_%d" % (o, s, bb, d))
+                    tg.setdefault(("Q", bb, "I", c), []).append("%s * %sad%d_%d" % (o, s, aa, d))
+                    tg.setdefault(("P", aa, "J", d), []).append("%s * %sbc%d_%d" % (o, s, bb, c))
+                    tg.setdefault(("Q", bb, "J", d), []).append("%s * %sac%d_%d" % (o, s, aa, c))
+            for (rs_, ri, cs_, ci), terms in tg.items():
+                em("atomicAdd(%s + (f%s + %d) * N + f%s + %d, deg * (%s));" % (acc, rs_, ri, cs_, ci, " + ".join(terms)))
+                qf += 2 * len(terms) + 1
+        em.ind -= 1
+        em("}")
+        fl["quartet"] += qf
+        em.ind -= 1
+        em("}")
+    em.ind -= 1
+    em("}")
+    # bra J: warp reduce (every lane shares the bra pair)
+    em("{")
+    em("  const int fP = bp.fP, fQ = bp.fQ;")
+    em("  const double s2 = 2.0 * deg;")
+    for ab in range(nab):
+        aa, bb = divmod(ab, nb_)
+        em("  { const double v = sqb::warp_sum(s2 * jab%d); if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(a.Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
+    em("}")
+    em("sqb::count_add(a.counters + 0, ok ? 1ull : 0ull);")
+    em("sqb::count_add(a.counters + 1, nprimq);")
+    em("sqb::count_add(a.counters + 2, nflush);")
+    out.extend(em.lines)
+    out.append("}")
+    meta = {"name": name, "bra": bra, "ket": ket, "spin": spin, "nab": nab, "ncd": ncd,
+            "neb": len(layb), "nek": len(layk), "Lt": Lt, "flops": fl}
+    return "\n".join(out) + "\n", meta
+
+
+def quartet_classes():
+    cls = []
+    for i, x in enumerate(PAIR_ORDER):
+        for y in PAIR_ORDER[: i + 1]:
+            cls.append((x, y))
+    return cls
+
+
+def main():
+    outdir = sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.path.dirname(__file__), "gen")
+    os.makedirs(outdir, exist_ok=True)
+    metas = []
+    files = []
+    for bra, ket in quartet_classes():
+        src = ['// generated by gen_jk_kernels.py -- do not edit', '#include "../jk_common.cuh"', '']
+        for spin in ("R", "U"):
+            s, m = gen_class(bra, ket, spin)
+            src.append(s)
+            metas.append(m)
+        fn = "jk_%s_%s.cu" % (bra, ket)
+        with open(os.path.join(outdir, fn), "w") as f:
+            f.write("\n".join(src))
+        files.append(fn)
+    # registry
+    reg = ['// generated by gen_jk_kernels.py -- do not edit', '#include "../jk_common.cuh"',
+           '#include "../jk_registry.h"', '']
+    for m in metas:
+        reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["name"])
+    reg.append("")
+    reg.append("namespace sqb {")
+    reg.append("const char* const kPairClassNames[%d] = {%s};" % (len(PAIRS), ", ".join('"%s"' % p for p in PAIRS)))
+    reg.append("const ClassKernel kClassKernels[%d] = {" % (len(metas) // 2))
+    for i in range(0, len(metas), 2):
+        r, u = metas[i], metas[i + 1]
+        reg.append('  {%d, %d, %d, %d, %d, %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+            PAIRS.index(r["bra"]), PAIRS.index(r["ket"]), r["nab"], r["ncd"], r["neb"], r["nek"],
+            r["Lt"], r["name"], u["name"], r["flops"]["prim"], r["flops"]["flush"], r["flops"]["quartet"]))
+    reg.append("};")
+    reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
+    reg.append("}  // namespace sqb")
+    with open(os.path.join(outdir, "jk_registry.cu"), "w") as f:
+        f.write("\n".join(reg) + "\n")
+    files.append("jk_registry.cu")
+    with open(os.path.join(outdir, "jk_flops.json"), "w") as f:
+        json.dump({m["name"]: m["flops"] for m in metas}, f, indent=0)
+    with open(os.path.join(outdir, "files.txt"), "w") as f:
+        f.write("\n".join(files) + "\n")
+    print("generated %d kernels in %d files" % (len(metas), len(files)))
+
+
+if __name__ == "__main__":
+    main()

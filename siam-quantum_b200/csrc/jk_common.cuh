@@ -1,0 +1,104 @@
+// Device-side records and the Boys function shared by every J/K class kernel.
+//
+// Boys function F_m(T) = int_0^1 u^(2m) exp(-T u^2) du  (role of fgamma_set, reference
+// src/fgamma.c:172-206).  Written from the mathematics, not from any library:
+//   T <  BOYS_TMAX : the top order F_M(T) by a 9-term Taylor expansion about the nearest grid
+//                    point T0 (spacing BOYS_H), F_M(T0+d) = sum_k F_{M+k}(T0) (-d)^k / k!,
+//                    then the stable downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1).
+//   T >= BOYS_TMAX : F_0 = sqrt(pi/T)/2 (the erfc tail is below 1e-17 relative there) and the
+//                    stable upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T).
+// The grid values are computed on the host in extended precision (boys_table.cpp).
+#pragma once
+#include <cstdint>
+
+#define BOYS_H      0.1
+#define BOYS_INV_H  10.0
+#define BOYS_TMAX   36.0
+#define BOYS_NGRID  361      // grid points T0 = 0, 0.1, ..., 36.0
+#define BOYS_MMAX   8        // highest order requested by a kernel ((dd|dd))
+#define BOYS_NTAY   9        // Taylor terms
+#define BOYS_NCOL   (BOYS_MMAX + BOYS_NTAY)   // columns m = 0..16 per grid row
+
+#define TWO_PI_2_5  34.986836655249725     // 2 pi^(5/2)
+#define PRIM_CUTOFF 1.0e-15                // reference src/int.h:19
+
+namespace sqb {
+
+// One shell pair (P >= Q in the reference's sorted shell order), 32 bytes.
+struct PairRec {
+  int P, Q;        // sorted shell indices
+  int fP, fQ;      // first basis function of each shell
+  int nprim;       // primitive pairs
+  int poff;        // offset (doubles) of the first primitive record in the class array
+  double schwarz;  // max over the block of the basis-level Schwarz matrix
+};
+
+// A CTA's unit of work: one bra pair and a contiguous range of ket pairs.
+struct WorkItem {
+  int bra, k0, cnt, pad;
+};
+
+struct JKArgs {
+  const PairRec* bra_pairs;
+  const double* bra_prims;
+  const PairRec* ket_pairs;
+  const double* ket_prims;
+  const double* PA;
+  const double* PB;
+  const double* PT;
+  const double* PM;            // ns x ns shell-block max of |PT|,|PA|,|PB|
+  double* Jacc;                // nbf x nbf, J = Jacc + Jacc^T
+  double* KAacc;               // nbf x nbf, K[PA] = KAacc + KAacc^T
+  double* KBacc;
+  const double* boys_tab;      // BOYS_NGRID x BOYS_NCOL
+  unsigned long long* counters;// [0] quartets computed, [1] primitive quartets evaluated
+  int nbf, ns;
+  int same_class;              // bra and ket pairs come from one class (pair identity possible)
+  int pad;
+  double cut_outer, cut_fixed, dscreen_rmax;
+};
+
+// F_0..F_M at T.  M is a compile-time order so the recursion unrolls.
+template <int M>
+__device__ __forceinline__ void boys(double T, const double* __restrict__ tab, double* F) {
+  if (T < BOYS_TMAX) {
+    const int g = __double2int_rn(T * BOYS_INV_H);
+    const double d = T - g * BOYS_H;          // |d| <= BOYS_H/2
+    const double* row = tab + g * BOYS_NCOL + M;
+    // Horner in -d with 1/k! folded in: sum_k row[k] (-d)^k / k!
+    double s = row[BOYS_NTAY - 1];
+#pragma unroll
+    for (int k = BOYS_NTAY - 2; k >= 0; --k) s = fma(s, -d / (double)(k + 1), row[k]);
+    F[M] = s;
+    if (M > 0) {
+      const double e = exp(-T);
+      const double t2 = T + T;
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));
+    }
+  } else {
+    const double it = 1.0 / T;
+    F[0] = 0.88622692545275801365 * sqrt(it);   // sqrt(pi)/2 / sqrt(T)
+    if (M > 0) {
+      const double e = exp(-T);
+      const double h = 0.5 * it;
+#pragma unroll
+      for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    }
+  }
+}
+
+// Warp-aggregated 64-bit counter increment.
+__device__ __forceinline__ void count_add(unsigned long long* c, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(c, v);
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace sqb

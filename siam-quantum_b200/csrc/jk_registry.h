@@ -1,0 +1,25 @@
+// Table of generated class kernels (filled in by gen/jk_registry.cu).
+#pragma once
+
+namespace sqb {
+
+// Pair classes in generator order: SS LS LL PS PL PP DS DL DP DD.
+constexpr int kNumPairClasses = 10;
+extern const char* const kPairClassNames[kNumPairClasses];
+
+struct ClassKernel {
+  int bra_cls, ket_cls;   // pair class of the CTA-shared bra and of the per-thread ket
+  int nab, ncd;           // functions per bra / ket pair
+  int neb, nek;           // Hermite E-table entries per primitive pair
+  int Lt;                 // total angular momentum
+  const void* fn_r;       // restricted kernel
+  const void* fn_u;       // unrestricted kernel
+  int flops_prim;         // FP64 ops per primitive quartet (all passes)
+  int flops_flush;        // FP64 ops per bra primitive and ket pair (all passes)
+  int flops_quartet;      // FP64 ops of the digestion per quartet
+};
+
+extern const ClassKernel kClassKernels[];
+extern const int kNumClassKernels;
+
+}  // namespace sqb

@@ -1,0 +1,125 @@
+"""Python binding of the B200 J/K engine (libsqb200.so, C ABI in include/sqb200.h).
+
+The engine runs only on the GPU: there is no CPU fallback.  Loading fails loudly when the
+shared library is missing, and building a context fails when no CUDA device is present.
+
+Mirrors the reference's Fock-build entry point GTO_JK_Matrix_Quartet_Parallel
+(src/matrix.c:3773) and its caller uhf_getGMatrix (src/uhf.c:112): given densities PA, PB it
+returns JT = J[PA+PB], KA = -K[PA], KB = -K[PB] (KB = KA when restricted), with the same
+Schwarz, density and primitive screening.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsqb200.so")
+
+_lib = None
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+
+EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_jk_build_device",
+           "sqb200_jk_stats", "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_last_error"]
+
+
+class SQB200Error(RuntimeError):
+    pass
+
+
+def load_library(path=LIB_PATH):
+    """Load libsqb200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise SQB200Error("libsqb200.so not built (%s); run `make -C siam-quantum_b200`" % path)
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.sqb200_jk_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, _i32p, _i32p, _f64p, _f64p,
+                                   _f64p, vp, ctypes.c_int]
+    L.sqb200_jk_destroy.argtypes = [vp]
+    L.sqb200_jk_build.argtypes = [vp, _f64p, _f64p, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                  ctypes.c_double, _f64p, _f64p, _f64p]
+    L.sqb200_jk_build_device.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, vp, vp, vp, vp]
+    L.sqb200_jk_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    L.sqb200_jk_schwarz.argtypes = [vp, _f64p]
+    L.sqb200_jk_mem_cutoff.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    L.sqb200_last_error.restype = ctypes.c_char_p
+    for name in EXPORTS:
+        getattr(L, name).restype = ctypes.c_int if name != "sqb200_last_error" else ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != 0:
+        raise SQB200Error("sqb200 error %d: %s" % (rc, _lib.sqb200_last_error().decode()))
+
+
+class JKEngine:
+    """Per-basis device context.  `basis` is a basis.Basis (flat genBasis-order arrays)."""
+
+    def __init__(self, basis, schwarz=None, device=0):
+        L = load_library()
+        self.nbf = basis.nbf
+        self._ctx = ctypes.c_void_p()
+        sch = None
+        if schwarz is not None:
+            self._sch = np.ascontiguousarray(schwarz, dtype=np.float64).reshape(-1)
+            sch = self._sch.ctypes.data_as(ctypes.c_void_p)
+        _check(L.sqb200_jk_create(ctypes.byref(self._ctx), basis.nbf, basis.nprim,
+                                  np.ascontiguousarray(basis.lmn.reshape(-1)),
+                                  np.ascontiguousarray(basis.center.reshape(-1)), basis.exps,
+                                  np.ascontiguousarray(basis.ncoef), sch, device))
+
+    def close(self):
+        if self._ctx:
+            _lib.sqb200_jk_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build(self, PA, PB=None, restricted=True, scf_cutoff=1e-10, fixed_cutoff=None,
+              dscreen_rmax=float("inf")):
+        """Host densities in, host JT, KA, KB out (synchronous)."""
+        n = self.nbf
+        PA = np.ascontiguousarray(PA, dtype=np.float64).reshape(n * n)
+        PBv = PA if PB is None else np.ascontiguousarray(PB, dtype=np.float64).reshape(n * n)
+        if fixed_cutoff is None:
+            fixed_cutoff = scf_cutoff
+        JT = np.empty(n * n); KA = np.empty(n * n); KB = np.empty(n * n)
+        _check(_lib.sqb200_jk_build(self._ctx, PA, PBv, int(bool(restricted)), scf_cutoff,
+                                    fixed_cutoff, dscreen_rmax, JT, KA, KB))
+        return JT.reshape(n, n), KA.reshape(n, n), KB.reshape(n, n)
+
+    def build_device(self, dPA, dPB, dJT, dKA, dKB=None, restricted=True, scf_cutoff=1e-10,
+                     fixed_cutoff=None, dscreen_rmax=float("inf"), stream=None):
+        """Device pointers (ints, e.g. torch tensor.data_ptr()) in and out; asynchronous."""
+        if fixed_cutoff is None:
+            fixed_cutoff = scf_cutoff
+        _check(_lib.sqb200_jk_build_device(self._ctx, dPA, dPB, int(bool(restricted)), scf_cutoff,
+                                           fixed_cutoff, dscreen_rmax, dJT, dKA, dKB, stream))
+
+    def stats(self):
+        """dict of the last build's counters."""
+        out = (ctypes.c_longlong * 5)()
+        _check(_lib.sqb200_jk_stats(self._ctx, out, 5))
+        return {"quartets": out[0], "prim_quartets": out[1], "flops": out[2], "shells": out[3],
+                "pairs": out[4]}
+
+    def mem_cutoff(self, fixed_cutoff, max_mem_mb):
+        v = ctypes.c_double()
+        _check(_lib.sqb200_jk_mem_cutoff(self._ctx, fixed_cutoff, int(max_mem_mb), ctypes.byref(v)))
+        return v.value
+
+    def schwarz(self):
+        S = np.empty(self.nbf * self.nbf)
+        _check(_lib.sqb200_jk_schwarz(self._ctx, S))
+        return S.reshape(self.nbf, self.nbf)

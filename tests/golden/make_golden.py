@@ -1,0 +1,106 @@
+"""Generate the golden fixtures of the J/K parity tests by running the REFERENCE itself.
+
+Runs oracle/_ref/sqref (the unmodified Siam Quantum 2 sources compiled by oracle/Makefile) on
+seeded synthetic molecules and stores, per case, in <case>.npz:
+  atoms (Z, x, y, z in angstrom), basis name,
+  the reference's own genBasis arrays (nprim, lmn, xyz in bohr, exps, coefs, norms),
+  the reference's basis-level Schwarz matrix (create_Schwarz),
+  the converged SCF energy and densities PA, PB (uhf(), -SCFACC=1STEP -SCFCONV=1e-8),
+  fresh reference J/K builds from the converged density at cutoff 1e-10:
+    *_mem  : -MAXMEM=250 (first visit computes every Schwarz survivor, no density screen)
+    *_dir  : -MAXMEM=0   (density screen on every quartet)
+Usage:  make -C oracle && python tests/golden/make_golden.py
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import port  # noqa: E402
+
+import importlib.util  # noqa: E402
+import types  # noqa: E402
+
+_pkg = types.ModuleType("sqb200")
+_pkg.__path__ = [os.path.join(ROOT, "siam-quantum_b200")]
+sys.modules.setdefault("sqb200", _pkg)
+from sqb200 import molecules as M  # noqa: E402
+
+BASIS_DIR = "/root/reference/basis"
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def hydroxyl():
+    """OH radical (doublet, UHF): O-H 0.97 angstrom along z."""
+    return [(8, 0.0, 0.0, 0.0), (1, 0.0, 0.0, 0.97)]
+
+
+def formaldehyde():
+    """H2CO, planar: C-O 1.21, C-H 1.10 angstrom, H-C-H 116.5 degrees."""
+    import math
+    a = math.radians(116.5 / 2)
+    return [(6, 0.0, 0.0, 0.0), (8, 0.0, 0.0, 1.21),
+            (1, 0.0, 1.10 * math.sin(a), -1.10 * math.cos(a)),
+            (1, 0.0, -1.10 * math.sin(a), -1.10 * math.cos(a))]
+
+
+CASES = [
+    ("water_321g", M.water, "321g", ()),
+    ("oh_321g_uhf", hydroxyl, "321g", ()),
+    ("h2co_631gs", formaldehyde, "631g_star", ()),
+    ("benzene_631gs", M.benzene, "631g_star", ()),
+]
+
+
+def ref_basis(xyz, bas):
+    r = subprocess.run([port.REF_BIN, "basis", xyz, bas], capture_output=True, text=True, check=True)
+    lines = r.stdout.splitlines()
+    i = 0
+    while True:   # the reference prints chatter first; the dump starts with a lone count
+        t = lines[i].split()
+        if len(t) == 1 and t[0].isdigit() and len(lines[i + 1].split()) == 7:
+            break
+        i += 1
+    n = int(lines[i]); i += 1
+    nprim, lmn, xyzs, exps, coefs, norms = [], [], [], [], [], []
+    for _ in range(n):
+        t = lines[i].split(); i += 1
+        nc = int(t[0])
+        nprim.append(nc); lmn.append([int(x) for x in t[1:4]]); xyzs.append([float(x) for x in t[4:7]])
+        for _k in range(nc):
+            e, c, nm = (float(x) for x in lines[i].split()); i += 1
+            exps.append(e); coefs.append(c); norms.append(nm)
+    return (np.array(nprim, np.int32), np.array(lmn, np.int32), np.array(xyzs), np.array(exps),
+            np.array(coefs), np.array(norms))
+
+
+def main():
+    for name, geom, bas, opts in CASES:
+        atoms = geom()
+        with tempfile.TemporaryDirectory() as d:
+            xyz = os.path.join(d, "m.xyz")
+            with open(xyz, "w") as f:
+                f.write(M.xyz_text(atoms, name))
+            bp = os.path.join(BASIS_DIR, bas + ".txt")
+            nprim, lmn, xyzs, exps, coefs, norms = ref_basis(xyz, bp)
+            n = len(nprim)
+            S = port.ref_schwarz(xyz, bp, n)
+            res, PA, PB = port.ref_scf(xyz, bp, ["-SCFACC=1STEP", "-SCFCONV=1e-8"] + list(opts))
+            restricted = bool(np.array_equal(PA, PB))
+            rec = dict(atoms=np.array(atoms), basis=bas, nprim=nprim, lmn=lmn, xyz=xyzs, exps=exps,
+                       coefs=coefs, norms=norms, schwarz=S, energy=res["energy"], PA=PA, PB=PB,
+                       restricted=restricted, cutoff=1e-10)
+            for tag, mm in (("mem", 250), ("dir", 0)):
+                JT, KA, KB, _ = port.ref_jk(xyz, bp, PA, None if restricted else PB,
+                                            restricted=restricted, cutoff=1e-10, max_mem=mm)
+                rec["JT_" + tag] = JT; rec["KA_" + tag] = KA; rec["KB_" + tag] = KB
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), **rec)
+        print(name, "nbf", n, "E", res["energy"], "restricted", restricted)
+
+
+if __name__ == "__main__":
+    main()
