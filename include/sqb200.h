@@ -64,8 +64,22 @@ int sqb200_jk_build_device(sqb200_jk *ctx, const double *dPA, const double *dPB,
 
 /* Counters of the last build: out[0] shell quartets computed, out[1] primitive quartets
  * evaluated, out[2] algorithmic FP64 operations (per-class operation table),
- * out[3] shells, out[4] shell pairs.  Synchronises the context stream. */
+ * out[3] shells, out[4] shell pairs, out[5] kernels the build enqueued.
+ * Synchronises the context stream.  (No reference counterpart: instrumentation.) */
 int sqb200_jk_stats(sqb200_jk *ctx, long long *out, int n);
+
+/* Per-class timing: enable (1) or disable (0) CUDA-event timing of every class kernel
+ * launch on the build's stream, clearing the accumulators.  (Instrumentation, no
+ * reference counterpart.) */
+int sqb200_jk_profile(sqb200_jk *ctx, int enable);
+
+/* Rows of 6 doubles per class kernel launched since sqb200_jk_profile(ctx, 1):
+ * [class index, launches, total ms, FP64 ops of the last build's launch, primitive
+ * quartets of that launch, shell quartets of that launch]; *nrows receives the count. */
+int sqb200_jk_profile_read(sqb200_jk *ctx, double *rows, int max_rows, int *nrows);
+
+/* "bra|ket" pair-class name of a class-kernel index, e.g. "LL|LS". */
+const char *sqb200_jk_class_name(int k);
 
 /* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,
  * src/matrix.c:389-440), written to the host array S (nbf*nbf). */
@@ -75,6 +89,12 @@ int sqb200_jk_schwarz(sqb200_jk *ctx, double *S);
  * in MB: the Schwarz product above which the reference's first visit skips the density
  * screen (pass it as dscreen_rmax to reproduce a first reference visit). */
 int sqb200_jk_mem_cutoff(sqb200_jk *ctx, double fixed_cutoff, int max_mem_mb, double *out);
+
+/* Non-tensor FMA throughput of `device` in TFLOP/s (FMA = 2 flops): 8 independent FP64
+ * (then FP32) FMA chains per thread, 8 CTAs x 256 threads per SM, `fp64_iters` x 16 steps
+ * per chain, timed with CUDA events.  The denominator for the roofline fraction of the
+ * J/K kernels, which run on the FP64 pipe.  (Instrumentation, no reference counterpart.) */
+int sqb200_peak_fma(int device, int fp64_iters, double *fp64_tflops, double *fp32_tflops);
 
 /* Text of the last error on this thread. */
 const char *sqb200_last_error(void);

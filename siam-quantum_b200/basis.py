@@ -103,3 +103,23 @@ def build_basis(atoms_bohr, name):
 
 def n_primitive_functions(b):
     return int(b.nprim.sum())
+
+
+_ELEMENT_NAMES = ["", "HYDROGEN", "HELIUM", "LITHIUM", "BERYLLIUM", "BORON", "CARBON", "NITROGEN",
+                  "OXYGEN", "FLUORINE", "NEON", "SODIUM", "MAGNESIUM", "ALUMINUM", "SILICON",
+                  "PHOSPHORUS", "SULFUR", "CHLORINE", "ARGON"]
+
+
+def gamess_text(name, elements):
+    """GAMESS-US basis text for the given atomic numbers (the format read_GAMESS_BasisSet,
+    src/basis.c:316, parses), so a CPU run of the reference can read the same tables."""
+    tab = basis_table(name)
+    lines = ["$DATA"]
+    for z in sorted(set(elements)):
+        lines.append(_ELEMENT_NAMES[z])
+        for kind, prims in tab[str(z)]:
+            lines.append("%s %d" % (kind, len(prims)))
+            for k, p in enumerate(prims):
+                lines.append("  %d " % (k + 1) + " ".join("%.10E" % v for v in p))
+    lines.append("$END")
+    return "\n".join(lines) + "\n"

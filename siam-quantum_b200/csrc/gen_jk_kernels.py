@@ -2,7 +2,9 @@
 
 One kernel per quartet class (bra pair class | ket pair class) and spin mode (R: restricted,
 K from PA only; U: unrestricted, K from PA and PB).  A CTA owns one bra shell pair and up to
-128 ket shell pairs (one shell quartet per thread).  For each quartet the thread evaluates
+128 ket shell pairs: one shell quartet per thread, or per `isplit` threads that each take a
+strided subset of the bra primitives (the digestion is linear, so each thread digests its
+partial contraction).  For each quartet the threads evaluate
 
     (ab|cd) = sum_{bra prims i} sum_{tuv} Eb_i[ab][tuv] *
               sum_{ket prims j} sum_{tau nu phi} (-1)^(tau+nu+phi) Ek_j[cd][tau nu phi] R_ij[t+tau, u+nu, v+phi]
@@ -11,8 +13,9 @@ where Eb/Ek are Hermite expansion coefficients (with contraction coefficients, e
 and 1/q folded in, precomputed per primitive pair on the host) and R are the Hermite Coulomb
 integrals built from the Boys function.  The inner sum over ket primitives is accumulated in
 Hermite space (G[cd][tuv]); the bra transform runs once per bra primitive.  When the per-thread
-state would not fit in registers the ket functions are processed in blocks ("passes"), each
-pass repeating the primitive loop.  The contracted block is digested at once into
+state would not fit in registers the ket functions are split into blocks ("passes"); each pass
+is a separate CTA (blockIdx.y) that repeats the primitive loop for its block.  The contracted
+block is digested at once into
 
     Jacc[ab] += 2 deg PT[cd] v     Jacc[cd] += 2 deg PT[ab] v
     Kacc[ac] += deg P[bd] v        Kacc[bc] += deg P[ad] v
@@ -160,13 +163,15 @@ def gen_class(bra, ket, spin):
     em("const int N = a.nbf;")
     em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
     em("__syncthreads();")
-    em("const int tid = threadIdx.x;")
-    em("bool ok = tid < it.cnt;")
+    em("const int isplit = it.isplit;                 // threads sharing one quartet (bra primitives split)")
+    em("const int kl = threadIdx.x / isplit, grp = threadIdx.x - kl * isplit;")
+    em("const int pass = blockIdx.y;                   // block of ket functions handled by this CTA")
+    em("bool ok = kl < it.cnt;")
     em("sqb::PairRec kp = bp;")
     em("double deg = 0.0;")
     em("if (ok) {")
     em.ind += 1
-    em("kp = a.ket_pairs[it.k0 + tid];")
+    em("kp = a.ket_pairs[it.k0 + kl];")
     em("const double r = bp.schwarz * kp.schwarz;")
     em("ok = !(r < a.cut_outer) && !(r < a.cut_fixed);")
     em("if (ok && r < a.dscreen_rmax) {")
@@ -176,7 +181,7 @@ def gen_class(bra, ket, spin):
     em("  const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];")
     em("  ok = !(r * mp < a.cut_fixed);")
     em("}")
-    em("deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + tid) ? 0.5 : 1.0);")
+    em("deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + kl) ? 0.5 : 1.0);")
     em.ind -= 1
     em("}")
     for ab in range(nab):
@@ -186,18 +191,19 @@ def gen_class(bra, ket, spin):
     em.ind += 1
     em("const double* __restrict__ kprim = a.ket_prims + kp.poff;")
     em("const int nbp = bp.nprim, nkp = kp.nprim;")
-    em("nflush = nbp;")
+    em("nflush = pass == 0 ? (unsigned long long)((nbp - grp + isplit - 1) / isplit) : 0ull;")
     em("const double* __restrict__ PA = a.PA;")
     if spin == "U":
         em("const double* __restrict__ PB = a.PB;")
     em("const double* __restrict__ PT = a.PT;")
+    em("switch (pass) {")
     for bi, blk in enumerate(blocks):
-        em("{  // pass %d: ket functions %s" % (bi, blk))
+        em("case %d: {  // ket functions %s" % (bi, blk))
         em.ind += 1
         for ab in range(nab):
             for cd in blk:
                 em("double o%d_%d = 0.0;" % (ab, cd))
-        em("for (int i = 0; i < nbp; ++i) {")
+        em("for (int i = grp; i < nbp; i += isplit) {")
         em.ind += 1
         em("const double* __restrict__ bi = sbra + i * %d;" % NB)
         em("const double p = bi[0], Px = bi[1], Py = bi[2], Pz = bi[3], kpb = bi[4];")
@@ -212,7 +218,7 @@ def gen_class(bra, ket, spin):
         em("const double rs = rsqrt(pq);")
         em("if (TWO_PI_2_5 * kpb * kj[4] * rs < PRIM_CUTOFF) continue;")
         if bi == 0:
-            em("++nprimq;")
+            em("++nprimq;")   # counted by the pass-0 CTAs only
         em("const double alpha = p * q * (rs * rs);")
         em("const double X = Px - kj[1], Y = Py - kj[2], Z = Pz - kj[3];")
         em("const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));")
@@ -319,7 +325,8 @@ def gen_class(bra, ket, spin):
         em("}")
         fl["quartet"] += qf
         em.ind -= 1
-        em("}")
+        em("} break;")
+    em("}")
     em.ind -= 1
     em("}")
     # bra J: warp reduce (every lane shares the bra pair)
@@ -330,9 +337,10 @@ def gen_class(bra, ket, spin):
         aa, bb = divmod(ab, nb_)
         em("  { const double v = sqb::warp_sum(s2 * jab%d); if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(a.Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
     em("}")
-    em("sqb::count_add(a.counters + 0, ok ? 1ull : 0ull);")
+    em("sqb::count_add(a.counters + 0, (ok && grp == 0 && pass == 0) ? 1ull : 0ull);")
     em("sqb::count_add(a.counters + 1, nprimq);")
     em("sqb::count_add(a.counters + 2, nflush);")
+    em("sqb::count_add(a.counters + 3, (ok && pass == 0) ? 1ull : 0ull);")
     out.extend(em.lines)
     out.append("}")
     meta = {"name": name, "bra": bra, "ket": ket, "spin": spin, "nab": nab, "ncd": ncd,
@@ -374,9 +382,10 @@ def main():
     reg.append("const ClassKernel kClassKernels[%d] = {" % (len(metas) // 2))
     for i in range(0, len(metas), 2):
         r, u = metas[i], metas[i + 1]
-        reg.append('  {%d, %d, %d, %d, %d, %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+        reg.append('  {%d, %d, %d, %d, %d, %d, %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
             PAIRS.index(r["bra"]), PAIRS.index(r["ket"]), r["nab"], r["ncd"], r["neb"], r["nek"],
-            r["Lt"], r["name"], u["name"], r["flops"]["prim"], r["flops"]["flush"], r["flops"]["quartet"]))
+            r["Lt"], r["flops"]["passes"], r["name"], u["name"], r["flops"]["prim"], r["flops"]["flush"],
+            r["flops"]["quartet"]))
     reg.append("};")
     reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
     reg.append("}  // namespace sqb")

@@ -7,7 +7,7 @@
 //                    then the stable downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1).
 //   T >= BOYS_TMAX : F_0 = sqrt(pi/T)/2 (the erfc tail is below 1e-17 relative there) and the
 //                    stable upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T).
-// The grid values are computed on the host in extended precision (boys_table.cpp).
+// The grid values are computed on the host in extended precision (jk_engine.cu).
 #pragma once
 #include <cstdint>
 
@@ -33,9 +33,10 @@ struct PairRec {
   double schwarz;  // max over the block of the basis-level Schwarz matrix
 };
 
-// A CTA's unit of work: one bra pair and a contiguous range of ket pairs.
+// A CTA's unit of work: one bra pair and a contiguous range of cnt ket pairs, each ket
+// handled by `isplit` threads (power of two) that split the bra primitives between them.
 struct WorkItem {
-  int bra, k0, cnt, pad;
+  int bra, k0, cnt, isplit;
 };
 
 struct JKArgs {
@@ -51,7 +52,8 @@ struct JKArgs {
   double* KAacc;               // nbf x nbf, K[PA] = KAacc + KAacc^T
   double* KBacc;
   const double* boys_tab;      // BOYS_NGRID x BOYS_NCOL
-  unsigned long long* counters;// [0] quartets computed, [1] primitive quartets evaluated
+  unsigned long long* counters;// [0] quartets computed, [1] primitive quartets evaluated,
+                               // [2] bra-primitive flushes, [3] digestions
   int nbf, ns;
   int same_class;              // bra and ket pairs come from one class (pair identity possible)
   int pad;
@@ -68,7 +70,7 @@ __device__ __forceinline__ void boys(double T, const double* __restrict__ tab, d
     // Horner in -d with 1/k! folded in: sum_k row[k] (-d)^k / k!
     double s = row[BOYS_NTAY - 1];
 #pragma unroll
-    for (int k = BOYS_NTAY - 2; k >= 0; --k) s = fma(s, -d / (double)(k + 1), row[k]);
+    for (int k = BOYS_NTAY - 2; k >= 0; --k) s = fma(s, -d * (1.0 / (double)(k + 1)), row[k]);
     F[M] = s;
     if (M > 0) {
       const double e = exp(-T);

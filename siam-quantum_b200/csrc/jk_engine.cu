@@ -174,7 +174,10 @@ int etable_size(int ta, int tb) {
 
 struct PairClass {
   int ta = -1, tb = -1, ne = 0, stride = 0, max_nprim = 0;
-  std::vector<sqb::PairRec> pairs;   // sorted by decreasing Schwarz bound
+  // sorted by primitive-pair count, then by decreasing Schwarz bound; sub[] holds the start
+  // of every run of equal primitive count (plus the end)
+  std::vector<sqb::PairRec> pairs;
+  std::vector<int> sub;
   std::vector<double> prims;
   sqb::PairRec* d_pairs = nullptr;
   double* d_prims = nullptr;
@@ -206,6 +209,13 @@ struct sqb200_jk {
   std::map<std::pair<double, double>, Work> work;
   std::vector<long long> last_counts;
   long long last_flops = 0;
+  int last_launches = 0;        // kernels enqueued by the last build
+  // per-class event timing (sqb200_jk_profile)
+  bool profile = false;
+  struct Ev { int kernel; cudaEvent_t a, b; };
+  std::vector<Ev> events;
+  std::vector<double> prof_ms;
+  std::vector<long long> prof_launches;
 };
 
 namespace {
@@ -253,6 +263,90 @@ __global__ void k_finalize(const double* __restrict__ J, const double* __restric
   }
 }
 
+// ---------------------------------------------------------------- Schwarz on the device
+//
+// sqrt|(ab|ab)| for every function pair of every shell pair (create_Schwarz, reference
+// src/matrix.c:389-440; contracted with no primitive cut, as its contr_eri), by the same
+// McMurchie-Davidson expansion: (ab|ab) = sum_{i,j} sum_{tuv,tau nu phi} E_i[tuv] E_j[tau nu phi]
+// (-1)^(tau+nu+phi) R_ij[t+tau, u+nu, v+phi].  One thread per (pair, a, b); runtime loops,
+// Hermite integrals in a per-thread tetrahedral table.
+
+struct SchwarzFn {
+  int nfn;
+  int sx[36], sy[36], sz[36], eoff[36];
+};
+
+__device__ __forceinline__ int tetra(int t, int u, int v) {
+  const int n = t + u + v, m = u + v;
+  return n * (n + 1) * (n + 2) / 6 + m * (m + 1) / 2 + v;
+}
+
+__global__ void k_schwarz(const sqb::PairRec* __restrict__ pairs, const double* __restrict__ prims, int npairs,
+                          int stride, int nfb, SchwarzFn fd, const double* __restrict__ tab, int nbf,
+                          double* __restrict__ S) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= npairs * fd.nfn) return;
+  const int pr = idx / fd.nfn, f = idx % fd.nfn;
+  const sqb::PairRec rec = pairs[pr];
+  const int sx = fd.sx[f], sy = fd.sy[f], sz = fd.sz[f], eo = fd.eoff[f];
+  const int L = 2 * (sx + sy + sz);
+  double acc = 0.0;
+  double Ra[165], Rb[165], F[9];
+  for (int i = 0; i < rec.nprim; ++i) {
+    const double* pi = prims + rec.poff + i * stride;
+    for (int j = 0; j < rec.nprim; ++j) {
+      const double* pj = prims + rec.poff + j * stride;
+      const double p = pi[0], q = pj[0], pq = p + q, rs = rsqrt(pq), alpha = p * q * (rs * rs);
+      const double X = pi[1] - pj[1], Y = pi[2] - pj[2], Z = pi[3] - pj[3];
+      const double T = alpha * (X * X + Y * Y + Z * Z);
+      sqb::boys<8>(T, tab, F);
+      // R^{(n)} from n = L down to 0
+      double* cur = Ra;
+      double* nxt = Rb;
+      const double s0 = TWO_PI_2_5 * rs;
+      double w = s0;
+      double base[9];
+      for (int n = 0; n <= L; ++n) { base[n] = w * F[n]; w *= -2.0 * alpha; }
+      cur[0] = base[L];
+      for (int n = L - 1; n >= 0; --n) {
+        const int top = L - n;
+        for (int N = 0; N <= top; ++N)
+          for (int t = N; t >= 0; --t)
+            for (int u = N - t; u >= 0; --u) {
+              const int v = N - t - u;
+              double r;
+              if (N == 0) r = base[n];
+              else if (t > 0) r = X * cur[tetra(t - 1, u, v)] + (t > 1 ? (t - 1) * cur[tetra(t - 2, u, v)] : 0.0);
+              else if (u > 0) r = Y * cur[tetra(t, u - 1, v)] + (u > 1 ? (u - 1) * cur[tetra(t, u - 2, v)] : 0.0);
+              else r = Z * cur[tetra(t, u, v - 1)] + (v > 1 ? (v - 1) * cur[tetra(t, u, v - 2)] : 0.0);
+              nxt[tetra(t, u, v)] = r;
+            }
+        double* tmp = cur; cur = nxt; nxt = tmp;
+      }
+      // contract with both E tables (same function pair)
+      int ka = 0;
+      for (int t = 0; t <= sx; ++t)
+        for (int u = 0; u <= sy; ++u)
+          for (int v = 0; v <= sz; ++v, ++ka) {
+            const double ea = pi[5 + eo + ka];
+            int kb = 0;
+            double s = 0.0;
+            for (int tt = 0; tt <= sx; ++tt)
+              for (int uu = 0; uu <= sy; ++uu)
+                for (int vv = 0; vv <= sz; ++vv, ++kb) {
+                  const double e = pj[5 + eo + kb];
+                  s += (((tt + uu + vv) & 1) ? -e : e) * cur[tetra(t + tt, u + uu, v + vv)];
+                }
+            acc += ea * s;
+          }
+    }
+  }
+  const int a = f / nfb, b = f % nfb;
+  const double v = sqrt(fabs(acc));
+  S[(size_t)(rec.fP + a) * nbf + rec.fQ + b] = v;
+  S[(size_t)(rec.fQ + b) * nbf + rec.fP + a] = v;
+}
+
 int grid_for(long n, int block) {
   long g = (n + block - 1) / block;
   return (int)std::min<long>(std::max<long>(g, 1), 148L * 16);
@@ -273,17 +367,21 @@ void build_pairs(sqb200_jk* c) {
       for (int q = 0; q < sh[Q].nfunc; ++q) r = std::max(r, c->schwarz[(size_t)(sh[P].first + p) * c->nbf + sh[Q].first + q]);
     return r;
   };
-  struct Tmp { double s; int P, Q; };
+  struct Tmp { double s; int P, Q, np; };
   std::vector<Tmp> lists[sqb::kNumPairClasses];
   for (int P = 0; P < ns; ++P)
     for (int Q = 0; Q <= P; ++Q) {
       const int k = pair_class_of(sh[P].type, sh[Q].type);
-      lists[k].push_back({sch(P, Q), P, Q});
+      lists[k].push_back({sch(P, Q), P, Q, sh[P].nprim * sh[Q].nprim});
     }
   for (int k = 0; k < sqb::kNumPairClasses; ++k) {
     PairClass& pc = c->cls[k];
-    std::stable_sort(lists[k].begin(), lists[k].end(), [](const Tmp& a, const Tmp& b) { return a.s > b.s; });
+    std::stable_sort(lists[k].begin(), lists[k].end(),
+                     [](const Tmp& a, const Tmp& b) { return a.np != b.np ? a.np < b.np : a.s > b.s; });
     if (lists[k].empty()) continue;
+    for (size_t i = 0; i < lists[k].size(); ++i)
+      if (i == 0 || lists[k][i].np != lists[k][i - 1].np) pc.sub.push_back((int)i);
+    pc.sub.push_back((int)lists[k].size());
     const Shell& s0 = sh[lists[k][0].P];
     const Shell& s1 = sh[lists[k][0].Q];
     pc.ta = s0.type;
@@ -330,6 +428,46 @@ void build_pairs(sqb200_jk* c) {
   }
 }
 
+int compute_schwarz_device(sqb200_jk* c, double* S_host) {
+  const size_t nn = (size_t)c->nbf * c->nbf;
+  double* dS = nullptr;
+  CUDA_OK(cudaMalloc(&dS, nn * sizeof(double)));
+  CUDA_OK(cudaMemset(dS, 0, nn * sizeof(double)));
+  for (int k = 0; k < sqb::kNumPairClasses; ++k) {
+    const PairClass& pc = c->cls[k];
+    if (pc.pairs.empty()) continue;
+    SchwarzFn fd;
+    memset(&fd, 0, sizeof(fd));
+    int off = 0;
+    for (int a = 0; a < kNComp[pc.ta]; ++a)
+      for (int b = 0; b < kNComp[pc.tb]; ++b) {
+        const int f = fd.nfn++;
+        fd.sx[f] = kComp[pc.ta][a][0] + kComp[pc.tb][b][0];
+        fd.sy[f] = kComp[pc.ta][a][1] + kComp[pc.tb][b][1];
+        fd.sz[f] = kComp[pc.ta][a][2] + kComp[pc.tb][b][2];
+        fd.eoff[f] = off;
+        off += (fd.sx[f] + 1) * (fd.sy[f] + 1) * (fd.sz[f] + 1);
+      }
+    const long nthr = (long)pc.pairs.size() * fd.nfn;
+    k_schwarz<<<(int)((nthr + 127) / 128), 128, 0, c->stream>>>(pc.d_pairs, pc.d_prims, (int)pc.pairs.size(), pc.stride,
+                                                               kNComp[pc.tb], fd, c->d_boys, c->nbf, dS);
+    CUDA_OK(cudaGetLastError());
+  }
+  CUDA_OK(cudaMemcpyAsync(S_host, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_OK(cudaStreamSynchronize(c->stream));
+  CUDA_OK(cudaFree(dS));
+  return SQB200_OK;
+}
+
+void free_pairs(sqb200_jk* c) {
+  for (int k = 0; k < sqb::kNumPairClasses; ++k) {
+    cudaFree(c->cls[k].d_pairs);
+    cudaFree(c->cls[k].d_prims);
+    c->cls[k].d_pairs = nullptr;
+    c->cls[k].d_prims = nullptr;
+  }
+}
+
 int upload_pairs(sqb200_jk* c) {
   for (int k = 0; k < sqb::kNumPairClasses; ++k) {
     PairClass& pc = c->cls[k];
@@ -360,20 +498,32 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
     if (B.pairs.empty() || T.pairs.empty()) continue;
     const int first = (int)items.size();
     const bool same = K.bra_cls == K.ket_cls;
-    for (int b = 0; b < (int)B.pairs.size(); ++b) {
-      const double sb = B.pairs[b].schwarz;
-      if (!(sb > 0.0)) break;   // sorted: the rest are zero
-      const double thr = cut / sb * (1.0 - 1e-12);
-      // ket pairs with schwarz >= thr form a prefix of the sorted class
-      int lo = 0, hi = (int)T.pairs.size();
-      while (lo < hi) {
-        const int mid = (lo + hi) / 2;
-        if (T.pairs[mid].schwarz >= thr) lo = mid + 1; else hi = mid;
+    // every (bra sub-list, ket sub-list) combination; inside one class each unordered pair of
+    // sub-lists once, and inside one sub-list each unordered pair of pairs once (k >= b)
+    for (size_t sx = 0; sx + 1 < B.sub.size(); ++sx)
+      for (size_t sy = 0; sy + 1 < T.sub.size(); ++sy) {
+        if (same && sx > sy) continue;
+        const int b0 = B.sub[sx], b1 = B.sub[sx + 1], k0s = T.sub[sy], k1s = T.sub[sy + 1];
+        const int nbp = B.pairs[b0].nprim, nkp = T.pairs[k0s].nprim;
+        // split the bra primitives over up to 32 threads when a quartet has many primitives
+        int isplit = 1;
+        while (isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
+        const int kper = 128 / isplit;
+        for (int b = b0; b < b1; ++b) {
+          const double sb = B.pairs[b].schwarz;
+          if (!(sb > 0.0)) break;   // sorted: the rest are zero
+          const double thr = cut / sb * (1.0 - 1e-12);
+          // ket pairs of the sub-list with schwarz >= thr form a prefix of it
+          int lo = k0s, hi = k1s;
+          while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if (T.pairs[mid].schwarz >= thr) lo = mid + 1; else hi = mid;
+          }
+          const int end = lo;
+          const int start = (same && sx == sy) ? b : k0s;
+          for (int k0 = start; k0 < end; k0 += kper) items.push_back({b, k0, std::min(kper, end - k0), isplit});
+        }
       }
-      const int end = lo;
-      const int start = same ? b : 0;
-      for (int k0 = start; k0 < end; k0 += 128) items.push_back({b, k0, std::min(128, end - k0), 0});
-    }
     const int cnt = (int)items.size() - first;
     if (cnt > 0) {
       w.kernel.push_back(ki);
@@ -402,7 +552,8 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   if (rc) return rc;
   k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf);
   k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM);
-  CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 3 * sqb::kNumClassKernels, st));
+  CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 4 * sqb::kNumClassKernels, st));
+  c->last_launches = 3 + (int)w->kernel.size();
   for (size_t s = 0; s < w->kernel.size(); ++s) {
     const sqb::ClassKernel& K = sqb::kClassKernels[w->kernel[s]];
     const PairClass& B = c->cls[K.bra_cls];
@@ -414,7 +565,7 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
     a.PA = dPA; a.PB = dPB; a.PT = c->d_PT; a.PM = c->d_PM;
     a.Jacc = c->d_J; a.KAacc = c->d_KA; a.KBacc = c->d_KB;
     a.boys_tab = c->d_boys;
-    a.counters = c->d_counters + 3 * w->kernel[s];
+    a.counters = c->d_counters + 4 * w->kernel[s];
     a.nbf = n; a.ns = c->ns;
     a.same_class = K.bra_cls == K.ket_cls;
     a.cut_outer = outer; a.cut_fixed = fixed; a.dscreen_rmax = dscreen;
@@ -423,7 +574,17 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
     const size_t smem = (size_t)B.max_nprim * B.stride * sizeof(double);
     const void* fn = uhf ? K.fn_u : K.fn_r;
     if (smem > 48 * 1024) CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    CUDA_OK(cudaLaunchKernel(fn, dim3(w->count[s]), dim3(128), args, smem, st));
+    sqb200_jk::Ev ev{w->kernel[s], nullptr, nullptr};
+    if (c->profile) {
+      CUDA_OK(cudaEventCreate(&ev.a));
+      CUDA_OK(cudaEventCreate(&ev.b));
+      CUDA_OK(cudaEventRecord(ev.a, st));
+    }
+    CUDA_OK(cudaLaunchKernel(fn, dim3(w->count[s], K.passes), dim3(128), args, smem, st));
+    if (c->profile) {
+      CUDA_OK(cudaEventRecord(ev.b, st));
+      c->events.push_back(ev);
+    }
   }
   k_finalize<<<grid_for(nn, 256), 256, 0, st>>>(c->d_J, c->d_KA, c->d_KB, dJT, dKA, dKB, n, uhf);
   CUDA_OK(cudaGetLastError());
@@ -452,12 +613,8 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   int rc = build_shells(nbf, nprim, lmn, xyz, exps, ncoefs, c->shells);
   if (rc) { delete c; return rc; }
   c->ns = (int)c->shells.size();
-  if (schwarz) {
-    c->schwarz.assign(schwarz, schwarz + (size_t)nbf * nbf);
-  } else {
-    delete c;
-    return fail(SQB200_EINVAL, "device Schwarz not yet available: pass the Schwarz matrix");
-  }
+  if (schwarz) c->schwarz.assign(schwarz, schwarz + (size_t)nbf * nbf);
+  else c->schwarz.assign((size_t)nbf * nbf, 1.0);   // placeholder until the device pass below
   build_pairs(c);
   rc = upload_pairs(c);
   if (rc) { sqb200_jk_destroy(c); return rc; }
@@ -479,13 +636,22 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   ALLOC(c->d_JT, nn * sizeof(double));
   ALLOC(c->d_KAo, nn * sizeof(double));
   ALLOC(c->d_KBo, nn * sizeof(double));
-  ALLOC(c->d_counters, 3 * sqb::kNumClassKernels * sizeof(unsigned long long));
+  ALLOC(c->d_counters, 4 * sqb::kNumClassKernels * sizeof(unsigned long long));
 #undef ALLOC
   cudaError_t e = cudaMemcpy(c->d_boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_shfirst, fst.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_shn, nf.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) { sqb200_jk_destroy(c); return fail(SQB200_ECUDA, cudaGetErrorString(e)); }
+  if (!schwarz) {
+    // Schwarz bounds from the device, then the pair lists in their final (sorted) order
+    rc = compute_schwarz_device(c, c->schwarz.data());
+    if (rc) { sqb200_jk_destroy(c); return rc; }
+    free_pairs(c);
+    build_pairs(c);
+    rc = upload_pairs(c);
+    if (rc) { sqb200_jk_destroy(c); return rc; }
+  }
   *out = c;
   return SQB200_OK;
 }
@@ -495,7 +661,8 @@ int sqb200_jk_destroy(sqb200_jk* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (auto& kv : c->work) cudaFree(kv.second.d_items);
-  for (int k = 0; k < sqb::kNumPairClasses; ++k) { cudaFree(c->cls[k].d_pairs); cudaFree(c->cls[k].d_prims); }
+  for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  free_pairs(c);
   void* ptrs[] = {c->d_boys, c->d_shfirst, c->d_shn, c->d_PA, c->d_PB, c->d_PT, c->d_PM, c->d_J, c->d_KA,
                   c->d_KB, c->d_JT, c->d_KAo, c->d_KBo, c->d_counters};
   for (void* p : ptrs) cudaFree(p);
@@ -536,25 +703,84 @@ int sqb200_jk_stats(sqb200_jk* c, long long* out, int n) {
   if (!c || !out) return fail(SQB200_EINVAL, "null argument");
   CUDA_OK(cudaSetDevice(c->device));
   CUDA_OK(cudaStreamSynchronize(c->stream));
-  std::vector<unsigned long long> h(3 * sqb::kNumClassKernels);
+  std::vector<unsigned long long> h(4 * sqb::kNumClassKernels);
   CUDA_OK(cudaMemcpy(h.data(), c->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   long long q = 0, pq = 0, fl = 0;
   for (int k = 0; k < sqb::kNumClassKernels; ++k) {
     const sqb::ClassKernel& K = sqb::kClassKernels[k];
-    q += (long long)h[3 * k];
-    pq += (long long)h[3 * k + 1];
-    fl += (long long)h[3 * k + 1] * K.flops_prim + (long long)h[3 * k + 2] * K.flops_flush +
-          (long long)h[3 * k] * K.flops_quartet;
+    q += (long long)h[4 * k];
+    pq += (long long)h[4 * k + 1];
+    fl += (long long)h[4 * k + 1] * K.flops_prim + (long long)h[4 * k + 2] * K.flops_flush +
+          (long long)h[4 * k + 3] * K.flops_quartet;
   }
-  long long v[5] = {q, pq, fl, (long long)c->ns, 0};
+  long long v[6] = {q, pq, fl, (long long)c->ns, 0, (long long)c->last_launches};
   for (int k = 0; k < sqb::kNumPairClasses; ++k) v[4] += (long long)c->cls[k].pairs.size();
-  for (int i = 0; i < n && i < 5; ++i) out[i] = v[i];
+  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
   return SQB200_OK;
 }
 
 int sqb200_jk_schwarz(sqb200_jk* c, double* S) {
   if (!c || !S) return fail(SQB200_EINVAL, "null argument");
-  return fail(SQB200_EINVAL, "device Schwarz not yet available");
+  CUDA_OK(cudaSetDevice(c->device));
+  return compute_schwarz_device(c, S);
+}
+
+int sqb200_jk_profile(sqb200_jk* c, int enable) {
+  if (!c) return fail(SQB200_EINVAL, "null argument");
+  CUDA_OK(cudaSetDevice(c->device));
+  CUDA_OK(cudaStreamSynchronize(c->stream));
+  for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+  c->events.clear();
+  c->prof_ms.assign(sqb::kNumClassKernels, 0.0);
+  c->prof_launches.assign(sqb::kNumClassKernels, 0);
+  c->profile = enable != 0;
+  return SQB200_OK;
+}
+
+int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows) {
+  if (!c || !rows || !nrows) return fail(SQB200_EINVAL, "null argument");
+  CUDA_OK(cudaSetDevice(c->device));
+  for (auto& e : c->events) {
+    CUDA_OK(cudaEventSynchronize(e.b));
+    float ms = 0.f;
+    CUDA_OK(cudaEventElapsedTime(&ms, e.a, e.b));
+    if (c->prof_ms.size() != (size_t)sqb::kNumClassKernels) {
+      c->prof_ms.assign(sqb::kNumClassKernels, 0.0);
+      c->prof_launches.assign(sqb::kNumClassKernels, 0);
+    }
+    c->prof_ms[e.kernel] += ms;
+    c->prof_launches[e.kernel] += 1;
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  c->events.clear();
+  std::vector<unsigned long long> h(4 * sqb::kNumClassKernels);
+  CUDA_OK(cudaMemcpy(h.data(), c->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  int r = 0;
+  for (int k = 0; k < sqb::kNumClassKernels && r < max_rows; ++k) {
+    if (c->prof_launches.empty() || c->prof_launches[k] == 0) continue;
+    const sqb::ClassKernel& K = sqb::kClassKernels[k];
+    double* row = rows + 6 * r;
+    row[0] = k;
+    row[1] = (double)c->prof_launches[k];
+    row[2] = c->prof_ms[k];
+    row[3] = (double)h[4 * k + 1] * K.flops_prim + (double)h[4 * k + 2] * K.flops_flush + (double)h[4 * k + 3] * K.flops_quartet;
+    row[4] = (double)h[4 * k + 1];
+    row[5] = (double)h[4 * k];
+    ++r;
+  }
+  *nrows = r;
+  return SQB200_OK;
+}
+
+const char* sqb200_jk_class_name(int k) {
+  if (k < 0 || k >= sqb::kNumClassKernels) return "";
+  static std::vector<std::string> names;
+  if (names.empty())
+    for (int i = 0; i < sqb::kNumClassKernels; ++i)
+      names.push_back(std::string(sqb::kPairClassNames[sqb::kClassKernels[i].bra_cls]) + "|" +
+                      sqb::kPairClassNames[sqb::kClassKernels[i].ket_cls]);
+  return names[k].c_str();
 }
 
 int sqb200_jk_mem_cutoff(sqb200_jk* c, double fixed, int max_mem_mb, double* out) {

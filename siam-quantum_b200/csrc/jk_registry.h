@@ -12,11 +12,12 @@ struct ClassKernel {
   int nab, ncd;           // functions per bra / ket pair
   int neb, nek;           // Hermite E-table entries per primitive pair
   int Lt;                 // total angular momentum
+  int passes;             // ket-function blocks = grid.y of a launch
   const void* fn_r;       // restricted kernel
   const void* fn_u;       // unrestricted kernel
   int flops_prim;         // FP64 ops per primitive quartet (all passes)
   int flops_flush;        // FP64 ops per bra primitive and ket pair (all passes)
-  int flops_quartet;      // FP64 ops of the digestion per quartet
+  int flops_quartet;      // FP64 ops of one digestion (all passes) of a (partial) quartet block
 };
 
 extern const ClassKernel kClassKernels[];

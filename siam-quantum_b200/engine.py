@@ -21,7 +21,8 @@ _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
 EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_jk_build_device",
-           "sqb200_jk_stats", "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_last_error"]
+           "sqb200_jk_stats", "sqb200_jk_profile", "sqb200_jk_profile_read", "sqb200_jk_class_name",
+           "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_peak_fma", "sqb200_last_error"]
 
 
 class SQB200Error(RuntimeError):
@@ -47,9 +48,15 @@ def load_library(path=LIB_PATH):
     L.sqb200_jk_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     L.sqb200_jk_schwarz.argtypes = [vp, _f64p]
     L.sqb200_jk_mem_cutoff.argtypes = [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
-    L.sqb200_last_error.restype = ctypes.c_char_p
+    L.sqb200_jk_profile.argtypes = [vp, ctypes.c_int]
+    L.sqb200_jk_profile_read.argtypes = [vp, _f64p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    L.sqb200_jk_class_name.argtypes = [ctypes.c_int]
+    L.sqb200_peak_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                  ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:
-        getattr(L, name).restype = ctypes.c_int if name != "sqb200_last_error" else ctypes.c_char_p
+        getattr(L, name).restype = ctypes.c_int
+    L.sqb200_last_error.restype = ctypes.c_char_p
+    L.sqb200_jk_class_name.restype = ctypes.c_char_p
     _lib = L
     return L
 
@@ -87,17 +94,20 @@ class JKEngine:
             pass
 
     def build(self, PA, PB=None, restricted=True, scf_cutoff=1e-10, fixed_cutoff=None,
-              dscreen_rmax=float("inf")):
-        """Host densities in, host JT, KA, KB out (synchronous)."""
+              dscreen_rmax=float("inf"), out=None):
+        """Host densities in, host JT, KA, KB out (synchronous).  `out` may supply three
+        preallocated C-contiguous float64 (n, n) arrays (e.g. pinned buffers)."""
         n = self.nbf
         PA = np.ascontiguousarray(PA, dtype=np.float64).reshape(n * n)
         PBv = PA if PB is None else np.ascontiguousarray(PB, dtype=np.float64).reshape(n * n)
         if fixed_cutoff is None:
             fixed_cutoff = scf_cutoff
-        JT = np.empty(n * n); KA = np.empty(n * n); KB = np.empty(n * n)
+        if out is None:
+            out = (np.empty((n, n)), np.empty((n, n)), np.empty((n, n)))
+        JT, KA, KB = (o.reshape(n * n) for o in out)
         _check(_lib.sqb200_jk_build(self._ctx, PA, PBv, int(bool(restricted)), scf_cutoff,
                                     fixed_cutoff, dscreen_rmax, JT, KA, KB))
-        return JT.reshape(n, n), KA.reshape(n, n), KB.reshape(n, n)
+        return out
 
     def build_device(self, dPA, dPB, dJT, dKA, dKB=None, restricted=True, scf_cutoff=1e-10,
                      fixed_cutoff=None, dscreen_rmax=float("inf"), stream=None):
@@ -109,10 +119,26 @@ class JKEngine:
 
     def stats(self):
         """dict of the last build's counters."""
-        out = (ctypes.c_longlong * 5)()
-        _check(_lib.sqb200_jk_stats(self._ctx, out, 5))
+        out = (ctypes.c_longlong * 6)()
+        _check(_lib.sqb200_jk_stats(self._ctx, out, 6))
         return {"quartets": out[0], "prim_quartets": out[1], "flops": out[2], "shells": out[3],
-                "pairs": out[4]}
+                "pairs": out[4], "launches": out[5]}
+
+    def profile(self, enable=True):
+        """Start (or stop) per-class CUDA-event timing of the class kernels."""
+        _check(_lib.sqb200_jk_profile(self._ctx, int(bool(enable))))
+
+    def profile_read(self):
+        """Per class kernel since profile(True): list of dicts (launches, ms, flops/launch, ...)."""
+        rows = np.zeros(6 * 200)
+        n = ctypes.c_int()
+        _check(_lib.sqb200_jk_profile_read(self._ctx, rows, 200, ctypes.byref(n)))
+        out = []
+        for r in rows[: 6 * n.value].reshape(-1, 6):
+            out.append({"class": _lib.sqb200_jk_class_name(int(r[0])).decode(), "launches": int(r[1]),
+                        "ms": float(r[2]), "flops": float(r[3]), "prim_quartets": int(r[4]),
+                        "quartets": int(r[5])})
+        return out
 
     def mem_cutoff(self, fixed_cutoff, max_mem_mb):
         v = ctypes.c_double()
@@ -123,3 +149,11 @@ class JKEngine:
         S = np.empty(self.nbf * self.nbf)
         _check(_lib.sqb200_jk_schwarz(self._ctx, S))
         return S.reshape(self.nbf, self.nbf)
+
+
+def peak_fma(device=0, iters=4096):
+    """Measured non-tensor FMA peaks (TFLOP/s) of the device: (fp64, fp32)."""
+    L = load_library()
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(L.sqb200_peak_fma(device, iters, ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value

@@ -111,22 +111,29 @@ def test_jk_device_api_with_torch_buffers():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_device_schwarz_matches_reference(case):
+    """sqrt|(pq|pq)| on the device against the reference's create_Schwarz."""
+    g = golden(case)
+    sqb = load_sqb200()
+    eng = sqb.JKEngine(golden_basis(g))          # no Schwarz given: computed on the device
+    S = eng.schwarz()
+    np.testing.assert_allclose(S, g["schwarz"], rtol=1e-12, atol=1e-14)
+    # and the build from device-computed bounds still matches the reference
+    JT, KA, _ = eng.build(g["PA"], None if g["restricted"] else g["PB"], restricted=bool(g["restricted"]),
+                          scf_cutoff=1e-10)
+    assert np.abs(JT - g["JT_dir"]).max() <= TOL
+    assert np.abs(KA - g["KA_dir"]).max() <= TOL
+
+
+@pytest.mark.gpu
 def test_c60_full_size_properties():
     """C60/6-31G (540 functions) at full size: outputs symmetric, J/K linear in the density
     (density screen off), and the Schwarz-survivor count matches the oracle's shell loop."""
     sqb = load_sqb200()
     atoms = sqb.molecules.to_bohr(sqb.molecules.c60())
     b = sqb.basis.build_basis(atoms, "631g")
-    S = port.schwarz(b) if False else None
-    # Schwarz from the oracle is minutes on one core; use the engine's device Schwarz when
-    # available, else the oracle's (skip the test if neither is quick).
-    try:
-        eng0 = sqb.JKEngine(b, schwarz=np.ones((b.nbf, b.nbf)))
-        S = eng0.schwarz()
-        eng0.close()
-    except sqb.SQB200Error:
-        pytest.skip("device Schwarz not available")
-    eng = sqb.JKEngine(b, schwarz=S)
+    eng = sqb.JKEngine(b)                        # device Schwarz
     n = b.nbf
     rng = np.random.default_rng(11)
     D1 = rng.normal(size=(n, n)) * 0.01; D1 = D1 + D1.T
@@ -137,3 +144,20 @@ def test_c60_full_size_properties():
     assert np.array_equal(J3, J3.T) and np.array_equal(K3, K3.T)
     assert np.abs(J3 - J1 - J2).max() < 1e-11 * max(1.0, np.abs(J3).max())
     assert np.abs(K3 - K1 - K2).max() < 1e-11 * max(1.0, np.abs(K3).max())
+    st = eng.stats()
+    assert st["shells"] == 180 and st["pairs"] == 180 * 181 // 2
+    # independent count of unordered shell-pair pairs with Sch(PQ)*Sch(IJ) >= 1e-10
+    S = eng.schwarz()
+    first, nf, _ = port.shells(b)
+    blk = np.array([[S[f0:f0 + n0, g0:g0 + m0].max() for g0, m0 in zip(first, nf)] for f0, n0 in zip(first, nf)])
+    pv = np.sort(np.concatenate([blk[P, :P + 1] for P in range(len(first))]))
+    cnt = 0
+    for i, v in enumerate(pv):   # pairs (i <= j) in sorted order with pv[i]*pv[j] >= cut
+        j0 = max(i, np.searchsorted(pv, 1e-10 / v if v > 0 else np.inf, side="left"))
+        while j0 > i and pv[j0 - 1] * v >= 1e-10:
+            j0 -= 1
+        while j0 < len(pv) and pv[j0] * v < 1e-10:
+            j0 += 1
+        cnt += len(pv) - max(j0, i)
+    assert st["quartets"] == cnt, (st["quartets"], cnt)
+    assert 30e6 < cnt < 40e6                     # survey: 36.2M survivors for C60/6-31G
