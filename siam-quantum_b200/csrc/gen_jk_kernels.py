@@ -48,7 +48,8 @@ TYPE_ID = {"S": 0, "L": 1, "P": 2, "D": 3}        # reference sort order (src/ma
 PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
 # bra/ket orientation: the larger pair (by functions, then L) is the bra
 PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
-STATE_MAX = 64          # doubles of G + out accumulators per pass
+STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out accumulators per pass
+PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
 CTA = 128
 
 
@@ -86,8 +87,10 @@ class Emitter:
         self.lines.append("  " * self.ind + s)
 
 
-def gen_R(em, L, need):
-    """Emit R^{(0)}_{tuv} for (t,u,v) in need; returns flop count and name map."""
+def gen_R(em, L, need, cons=None, emit_use=None):
+    """Emit R^{(0)}_{tuv} for (t,u,v) in need; returns flop count and name map.  When
+    emit_use is given it is called right after each R^{(0)} value is produced, so its
+    consumers follow it and the value dies early (lower register pressure)."""
     have = {}
     flops = [0]
 
@@ -126,6 +129,8 @@ def gen_R(em, L, need):
     names = {}
     for (t, u, v) in sorted(need, key=lambda x: (sum(x), x)):
         names[(t, u, v)] = get(0, t, u, v)
+        if emit_use is not None:
+            emit_use((t, u, v), names[(t, u, v)])
     return names, flops[0]
 
 
@@ -210,47 +215,81 @@ def gen_class(bra, ket, spin):
         for cd in blk:
             for h in Hb:
                 em("double g%d_%d = 0.0;" % (cd, hidx[h]))
+        # ket E-table entries this block reads
+        kent = []
+        for cd in blk:
+            for k, (tau, nu, phi) in enumerate(nz(fk[cd])):
+                kent.append((cd, k, offk[cd] + k, -1 if (tau + nu + phi) % 2 else 1))
+        if PREFETCH:
+            # two-stage software pipeline: the record of primitive j+1 is loaded while j is
+            # computed, and its Boys-table row is fetched at the end of iteration j
+            em("double nq = 0.0, nQx = 0.0, nQy = 0.0, nQz = 0.0, nkq = 0.0;")
+            for (cd, k, e, sg) in kent:
+                em("double nek%d_%d = 0.0;" % (cd, k))
+            em("if (nkp > 0) { nq = kprim[0]; nQx = kprim[1]; nQy = kprim[2]; nQz = kprim[3]; nkq = kprim[4];")
+            for (cd, k, e, sg) in kent:
+                em("  nek%d_%d = %skprim[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
+            em("}")
         em("for (int j = 0; j < nkp; ++j) {")
         em.ind += 1
-        em("const double* __restrict__ kj = kprim + j * %d;" % NK)
-        em("const double q = kj[0];")
-        em("const double pq = p + q;")
-        em("const double rs = rsqrt(pq);")
-        em("if (TWO_PI_2_5 * kpb * kj[4] * rs < PRIM_CUTOFF) continue;")
+        if PREFETCH:
+            em("const double q = nq, Qx = nQx, Qy = nQy, Qz = nQz, kq = nkq;")
+            for (cd, k, e, sg) in kent:
+                em("const double ek%d_%d = nek%d_%d;" % (cd, k, cd, k))
+            em("if (j + 1 < nkp) { const double* __restrict__ kn = kprim + (j + 1) * %d;" % NK)
+            em("  nq = kn[0]; nQx = kn[1]; nQy = kn[2]; nQz = kn[3]; nkq = kn[4];")
+            for (cd, k, e, sg) in kent:
+                em("  nek%d_%d = %skn[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
+            em("}")
+            em("const double pq = p + q;")
+            em("const double rs = rsqrt(pq);")
+            em("if (TWO_PI_2_5 * kpb * kq * rs < PRIM_CUTOFF) continue;")
+        else:
+            em("const double* __restrict__ kj = kprim + j * %d;" % NK)
+            em("const double q = kj[0];")
+            em("const double pq = p + q;")
+            em("const double rs = rsqrt(pq);")
+            em("if (TWO_PI_2_5 * kpb * kj[4] * rs < PRIM_CUTOFF) continue;")
         if bi == 0:
             em("++nprimq;")   # counted by the pass-0 CTAs only
         em("const double alpha = p * q * (rs * rs);")
-        em("const double X = Px - kj[1], Y = Py - kj[2], Z = Pz - kj[3];")
+        if PREFETCH:
+            em("const double X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;")
+        else:
+            em("const double X = Px - kj[1], Y = Py - kj[2], Z = Pz - kj[3];")
         em("const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));")
-        em("double F[%d];" % (Lt + 1))
-        em("sqb::boys<%d>(T, a.boys_tab, F);" % Lt)
-        em("const double s0 = TWO_PI_2_5 * rs;")
-        em("const double m2a = -2.0 * alpha;")
-        em("double w = s0;")
-        pf = 9 + 2 + 3 + 5 + boys_flops(Lt) + 2  # setup: pq, alpha, XYZ diff, T, s0, m2a
-        for n in range(Lt + 1):
-            if n > 0:
-                em("w *= m2a;")
-                pf += 1
-            em("const double b%d = w * F[%d];" % (n, n))
-            pf += 1
         need = set()
         for cd in blk:
             for (tau, nu, phi) in nz(fk[cd]):
                 for h in Hb:
                     need.add((h[0] + tau, h[1] + nu, h[2] + phi))
-        rn, rf = gen_R(em, Lt, need)
-        pf += rf
+        Lp = max(sum(x) for x in need)          # highest Hermite order this pass needs
+        em("double F[%d];" % (Lp + 1))
+        em("sqb::boys<%d>(T, a.boys_tab, F);" % Lp)
+        em("const double s0 = TWO_PI_2_5 * rs;")
+        em("const double m2a = -2.0 * alpha;")
+        em("double w = s0;")
+        pf = 9 + 2 + 3 + 5 + boys_flops(Lp) + 2  # setup: pq, alpha, XYZ diff, T, s0, m2a
+        for n in range(Lp + 1):
+            if n > 0:
+                em("w *= m2a;")
+                pf += 1
+            em("const double b%d = w * F[%d];" % (n, n))
+            pf += 1
+        # ket E coefficients of this block, signed by (-1)^(tau+nu+phi)
+        if not PREFETCH:
+            for (cd, k, e, sg) in kent:
+                em("const double ek%d_%d = %skj[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
+        # consumers of each R value: (cd, k, h) with h + (tau nu phi) = R index
+        cons = {}
         for cd in blk:
             for k, (tau, nu, phi) in enumerate(nz(fk[cd])):
-                e = offk[cd] + k
-                sign = -1 if (tau + nu + phi) % 2 else 1
-                em("{ const double ek = %skj[%d];" % ("-" if sign < 0 else "", 5 + e))
                 for h in Hb:
-                    rr = rn[(h[0] + tau, h[1] + nu, h[2] + phi)]
-                    em("  g%d_%d = fma(ek, %s, g%d_%d);" % (cd, hidx[h], rr, cd, hidx[h]))
-                    pf += 2
-                em("}")
+                    cons.setdefault((h[0] + tau, h[1] + nu, h[2] + phi), []).append((cd, k, h))
+        rn, rf = gen_R(em, Lp, need, cons=cons, emit_use=lambda key, name: [
+            (em("g%d_%d = fma(ek%d_%d, %s, g%d_%d);" % (cd, hidx[h], cd, k, name, cd, hidx[h])))
+            for (cd, k, h) in cons.get(key, [])])
+        pf += rf + 2 * sum(len(v) for v in cons.values())
         em.ind -= 1
         em("}")
         # flush: o[ab][cd] += sum_h Eb[ab][h] g[cd][h]
@@ -348,6 +387,13 @@ def gen_class(bra, ket, spin):
     return "\n".join(out) + "\n", meta
 
 
+def write_if_changed(path, text):
+    if os.path.exists(path) and open(path).read() == text:
+        return
+    with open(path, "w") as f:
+        f.write(text)
+
+
 def quartet_classes():
     cls = []
     for i, x in enumerate(PAIR_ORDER):
@@ -368,8 +414,7 @@ def main():
             src.append(s)
             metas.append(m)
         fn = "jk_%s_%s.cu" % (bra, ket)
-        with open(os.path.join(outdir, fn), "w") as f:
-            f.write("\n".join(src))
+        write_if_changed(os.path.join(outdir, fn), "\n".join(src))
         files.append(fn)
     # registry
     reg = ['// generated by gen_jk_kernels.py -- do not edit', '#include "../jk_common.cuh"',
@@ -389,13 +434,11 @@ def main():
     reg.append("};")
     reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
     reg.append("}  // namespace sqb")
-    with open(os.path.join(outdir, "jk_registry.cu"), "w") as f:
-        f.write("\n".join(reg) + "\n")
+    write_if_changed(os.path.join(outdir, "jk_registry.cu"), "\n".join(reg) + "\n")
     files.append("jk_registry.cu")
-    with open(os.path.join(outdir, "jk_flops.json"), "w") as f:
-        json.dump({m["name"]: m["flops"] for m in metas}, f, indent=0)
-    with open(os.path.join(outdir, "files.txt"), "w") as f:
-        f.write("\n".join(files) + "\n")
+    write_if_changed(os.path.join(outdir, "jk_flops.json"),
+                     json.dumps({m["name"]: m["flops"] for m in metas}, indent=0))
+    write_if_changed(os.path.join(outdir, "files.txt"), "\n".join(files) + "\n")
     print("generated %d kernels in %d files" % (len(metas), len(files)))
 
 
