@@ -50,6 +50,7 @@ PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
 PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
 STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out accumulators per pass
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
+USE_WS = int(os.environ.get("SQB_WS", "0"))   # also emit warp-specialised multi-pass kernels (measured slower on B200; opt-in)
 CTA = 128
 
 
@@ -307,61 +308,7 @@ def gen_class(bra, ket, spin):
         fl["prim"] += pf
         fl["flush"] += ff
         # digestion of this block
-        qf = 0
-        cset = sorted({cd // nd for cd in blk})
-        dset = sorted({cd % nd for cd in blk})
-        em("{  // digest")
-        em.ind += 1
-        em("const int fP = bp.fP, fQ = bp.fQ, fI = kp.fP, fJ = kp.fQ;")
-        # densities needed
-        for cd in blk:
-            c, d = divmod(cd, nd)
-            em("const double ptk%d = PT[(fI + %d) * N + fJ + %d];" % (cd, c, d))
-        for ab in range(nab):
-            aa, bb = divmod(ab, nb_)
-            em("const double ptb%d = PT[(fP + %d) * N + fQ + %d];" % (ab, aa, bb))
-        spins = [("A", "PA")] + ([("B", "PB")] if spin == "U" else [])
-        for s, P_ in spins:
-            for bb in range(nb_):
-                for d in dset:
-                    em("const double %sbd%d_%d = %s[(fQ + %d) * N + fJ + %d];" % (s, bb, d, P_, bb, d))
-            for aa in range(na):
-                for d in dset:
-                    em("const double %sad%d_%d = %s[(fP + %d) * N + fJ + %d];" % (s, aa, d, P_, aa, d))
-            for bb in range(nb_):
-                for c in cset:
-                    em("const double %sbc%d_%d = %s[(fQ + %d) * N + fI + %d];" % (s, bb, c, P_, bb, c))
-            for aa in range(na):
-                for c in cset:
-                    em("const double %sac%d_%d = %s[(fP + %d) * N + fI + %d];" % (s, aa, c, P_, aa, c))
-        # J
-        for ab in range(nab):
-            terms = " + ".join("o%d_%d * ptk%d" % (ab, cd, cd) for cd in blk)
-            em("jab%d += %s;" % (ab, terms))
-            qf += 2 * len(blk)
-        for cd in blk:
-            c, d = divmod(cd, nd)
-            terms = " + ".join("o%d_%d * ptb%d" % (ab, cd, ab) for ab in range(nab))
-            em("atomicAdd(a.Jacc + (fI + %d) * N + fJ + %d, 2.0 * deg * (%s));" % (c, d, terms))
-            qf += 2 * nab + 2
-        # K
-        for s, _ in spins:
-            acc = "a.KAacc" if s == "A" else "a.KBacc"
-            tg = {}
-            for ab in range(nab):
-                aa, bb = divmod(ab, nb_)
-                for cd in blk:
-                    c, d = divmod(cd, nd)
-                    o = "o%d_%d" % (ab, cd)
-                    tg.setdefault(("P", aa, "I", c), []).append("%s * %sbd%d_%d" % (o, s, bb, d))
-                    tg.setdefault(("Q", bb, "I", c), []).append("%s * %sad%d_%d" % (o, s, aa, d))
-                    tg.setdefault(("P", aa, "J", d), []).append("%s * %sbc%d_%d" % (o, s, bb, c))
-                    tg.setdefault(("Q", bb, "J", d), []).append("%s * %sac%d_%d" % (o, s, aa, c))
-            for (rs_, ri, cs_, ci), terms in tg.items():
-                em("atomicAdd(%s + (f%s + %d) * N + f%s + %d, deg * (%s));" % (acc, rs_, ri, cs_, ci, " + ".join(terms)))
-                qf += 2 * len(terms) + 1
-        em.ind -= 1
-        em("}")
+        qf = emit_digest(em, spin, blk, nab, na, nb_, nd)
         fl["quartet"] += qf
         em.ind -= 1
         em("} break;")
@@ -385,6 +332,283 @@ def gen_class(bra, ket, spin):
     meta = {"name": name, "bra": bra, "ket": ket, "spin": spin, "nab": nab, "ncd": ncd,
             "neb": len(layb), "nek": len(layk), "Lt": Lt, "flops": fl}
     return "\n".join(out) + "\n", meta
+
+
+def emit_digest(em, spin, blk, nab, na, nb_, nd):
+    """Digest the contracted block o<ab>_<cd> (cd in blk) into the J/K accumulators.
+    Expects PA, PB (unrestricted), PT, N, bp, kp, deg and jab<ab> in scope; returns flops."""
+    qf = 0
+    cset = sorted({cd // nd for cd in blk})
+    dset = sorted({cd % nd for cd in blk})
+    em("{  // digest")
+    em.ind += 1
+    em("const int fP = bp.fP, fQ = bp.fQ, fI = kp.fP, fJ = kp.fQ;")
+    for cd in blk:
+        c, d = divmod(cd, nd)
+        em("const double ptk%d = PT[(fI + %d) * N + fJ + %d];" % (cd, c, d))
+    for ab in range(nab):
+        aa, bb = divmod(ab, nb_)
+        em("const double ptb%d = PT[(fP + %d) * N + fQ + %d];" % (ab, aa, bb))
+    spins = [("A", "PA")] + ([("B", "PB")] if spin == "U" else [])
+    for s, P_ in spins:
+        for bb in range(nb_):
+            for d in dset:
+                em("const double %sbd%d_%d = %s[(fQ + %d) * N + fJ + %d];" % (s, bb, d, P_, bb, d))
+        for aa in range(na):
+            for d in dset:
+                em("const double %sad%d_%d = %s[(fP + %d) * N + fJ + %d];" % (s, aa, d, P_, aa, d))
+        for bb in range(nb_):
+            for c in cset:
+                em("const double %sbc%d_%d = %s[(fQ + %d) * N + fI + %d];" % (s, bb, c, P_, bb, c))
+        for aa in range(na):
+            for c in cset:
+                em("const double %sac%d_%d = %s[(fP + %d) * N + fI + %d];" % (s, aa, c, P_, aa, c))
+    for ab in range(nab):
+        terms = " + ".join("o%d_%d * ptk%d" % (ab, cd, cd) for cd in blk)
+        em("jab%d += %s;" % (ab, terms))
+        qf += 2 * len(blk)
+    for cd in blk:
+        c, d = divmod(cd, nd)
+        terms = " + ".join("o%d_%d * ptb%d" % (ab, cd, ab) for ab in range(nab))
+        em("atomicAdd(a.Jacc + (fI + %d) * N + fJ + %d, 2.0 * deg * (%s));" % (c, d, terms))
+        qf += 2 * nab + 2
+    for s, _ in spins:
+        acc = "a.KAacc" if s == "A" else "a.KBacc"
+        tg = {}
+        for ab in range(nab):
+            aa, bb = divmod(ab, nb_)
+            for cd in blk:
+                c, d = divmod(cd, nd)
+                o = "o%d_%d" % (ab, cd)
+                tg.setdefault(("P", aa, "I", c), []).append("%s * %sbd%d_%d" % (o, s, bb, d))
+                tg.setdefault(("Q", bb, "I", c), []).append("%s * %sad%d_%d" % (o, s, aa, d))
+                tg.setdefault(("P", aa, "J", d), []).append("%s * %sbc%d_%d" % (o, s, bb, c))
+                tg.setdefault(("Q", bb, "J", d), []).append("%s * %sac%d_%d" % (o, s, aa, c))
+        for (rs_, ri, cs_, ci), terms in tg.items():
+            em("atomicAdd(%s + (f%s + %d) * N + f%s + %d, deg * (%s));" % (acc, rs_, ri, cs_, ci, " + ".join(terms)))
+            qf += 2 * len(terms) + 1
+    em.ind -= 1
+    em("}")
+    return qf
+
+
+WS_SMEM_MAX = 100 * 1024     # shared-memory budget of the R staging buffer
+
+
+def ws_plan(bra, ket):
+    """(passes, ket blocks, R list) of the warp-specialised form, or None if it does not fit."""
+    fb, offb, layb = etable(bra)
+    fk, offk, layk = etable(ket)
+    nab, ncd = len(fb), len(fk)
+    Hb = sorted({h for f in fb for h in nz(f)}, key=lambda x: (sum(x), x))
+    per = max(1, STATE_MAX // (len(Hb) + nab))
+    blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
+    P = len(blocks)
+    need = sorted({(h[0] + t, h[1] + u, h[2] + v) for cd in range(ncd) for (t, u, v) in nz(fk[cd]) for h in Hb},
+                  key=lambda x: (sum(x), x))
+    if P < 2 or P > 16 or P * len(need) * 32 * 8 > WS_SMEM_MAX:
+        return None
+    return P, blocks, need
+
+
+def gen_class_ws(bra, ket, spin):
+    """Warp-specialised form for multi-pass classes: one CTA = P warps = P ket-function blocks
+    for the same 32 ket pairs (lane = ket).  Each round, warp w evaluates the Boys function and
+    the Hermite integrals R of primitive step r0+w for its lane's quartet into shared memory;
+    after a barrier every warp consumes the P staged steps for its own block.  R is therefore
+    computed once per primitive quartet instead of once per block."""
+    P, blocks, need = ws_plan(bra, ket)
+    fb, offb, layb = etable(bra)
+    fk, offk, layk = etable(ket)
+    nab, ncd = len(fb), len(fk)
+    Hb = sorted({h for f in fb for h in nz(f)}, key=lambda x: (sum(x), x))
+    hidx = {h: i for i, h in enumerate(Hb)}
+    na, nb_ = len(COMP[bra[0]]), len(COMP[bra[1]])
+    nd = len(COMP[ket[1]])
+    NB = 5 + len(layb)
+    NK = 5 + len(layk)
+    NR = len(need)
+    ridx = {r: i for i, r in enumerate(need)}
+    Lm = max(sum(x) for x in need)
+    NT = 32 * P
+    name = "jk_%s_%s_%s_ws" % (bra, ket, spin)
+    fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": P, "nr": NR}
+    em = Emitter()
+    out = ['extern "C" __global__ void __launch_bounds__(%d)' % NT,
+           "%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name]
+    em("extern __shared__ double smem[];")
+    em("double* __restrict__ sR = smem;                       // [%d steps][%d R][32 lanes]" % (P, NR))
+    em("double* __restrict__ sbra = smem + %d;" % (P * NR * 32))
+    em("const sqb::WorkItem it = items[blockIdx.x];")
+    em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
+    em("const int N = a.nbf;")
+    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
+    em("__syncthreads();")
+    em("const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;")
+    em("bool ok = lane < it.cnt;")
+    em("const sqb::PairRec kp = a.ket_pairs[it.k0 + (ok ? lane : 0)];   // idle lanes shadow the first ket")
+    em("double deg = 0.0;")
+    em("if (ok) {")
+    em("  const double r = bp.schwarz * kp.schwarz;")
+    em("  ok = !(r < a.cut_outer) && !(r < a.cut_fixed);")
+    em("  if (ok && r < a.dscreen_rmax) {")
+    em("    const bool bf = (bp.P > kp.P) || (bp.P == kp.P && bp.Q >= kp.Q);")
+    em("    const int P = bf ? bp.P : kp.P, Q = bf ? bp.Q : kp.Q, I = bf ? kp.P : bp.P, J = bf ? kp.Q : bp.Q;")
+    em("    const double* PM = a.PM; const int ns = a.ns;")
+    em("    const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];")
+    em("    ok = !(r * mp < a.cut_fixed);")
+    em("  }")
+    em("  deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + lane) ? 0.5 : 1.0);")
+    em("}")
+    em("const int nbp = bp.nprim, nkp = kp.nprim, S = nbp * nkp;   // uniform over the CTA")
+    em("const double* __restrict__ kprim = a.ket_prims + kp.poff;")
+    em("const double* __restrict__ PA = a.PA;")
+    if spin == "U":
+        em("const double* __restrict__ PB = a.PB;")
+    em("const double* __restrict__ PT = a.PT;")
+    for ab in range(nab):
+        em("double jab%d = 0.0;" % ab)
+    em("unsigned long long nprimq = 0;")
+    prod = Emitter()
+    prod.ind = 0
+    prod("{  // produce primitive step r0 + wp")
+    prod.ind += 1
+    prod("const int s = r0 + wp;")
+    prod("if (s < S) {")
+    prod.ind += 1
+    prod("double* __restrict__ dst = sR + wp * %d + lane;" % (NR * 32))
+    prod("const int i = s / nkp, j = s - i * nkp;")
+    prod("const double* __restrict__ bi = sbra + i * %d;" % NB)
+    prod("const double* __restrict__ kj = kprim + j * %d;" % NK)
+    prod("const double p = bi[0], q = kj[0];")
+    prod("const double pq = p + q;")
+    prod("const double rs = rsqrt(pq);")
+    prod("if (TWO_PI_2_5 * bi[4] * kj[4] * rs < PRIM_CUTOFF) {")
+    for k in range(NR):
+        prod("  dst[%d] = 0.0;" % (32 * k))
+    prod("} else {")
+    prod.ind += 1
+    prod("if (ok) ++nprimq;")
+    prod("const double alpha = p * q * (rs * rs);")
+    prod("const double X = bi[1] - kj[1], Y = bi[2] - kj[2], Z = bi[3] - kj[3];")
+    prod("const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));")
+    prod("double F[%d];" % (Lm + 1))
+    prod("sqb::boys<%d>(T, a.boys_tab, F);" % Lm)
+    prod("const double m2a = -2.0 * alpha;")
+    prod("double w = TWO_PI_2_5 * rs;")
+    pf = 9 + 2 + 3 + 5 + boys_flops(Lm) + 2
+    for n in range(Lm + 1):
+        if n > 0:
+            prod("w *= m2a;")
+            pf += 1
+        prod("const double b%d = w * F[%d];" % (n, n))
+        pf += 1
+    rn, rf = gen_R(prod, Lm, set(need), emit_use=lambda key, nm: prod("dst[%d] = %s;" % (32 * ridx[key], nm)))
+    pf += rf
+    prod.ind -= 1
+    prod("}")
+    prod.ind -= 1
+    prod("}")
+    prod.ind -= 1
+    prod("}")
+    em("switch (wp) {")
+    for bi_, blk in enumerate(blocks):
+        em("case %d: {  // ket functions %s" % (bi_, blk))
+        em.ind += 1
+        for ab in range(nab):
+            for cd in blk:
+                em("double o%d_%d = 0.0;" % (ab, cd))
+        for cd in blk:
+            for h in Hb:
+                em("double g%d_%d = 0.0;" % (cd, hidx[h]))
+        em("int cur = 0;")
+        em("for (int r0 = 0; r0 < S; r0 += %d) {" % P)
+        em.ind += 1
+        for line in prod.lines:
+            em(line)
+        em('asm volatile("bar.sync 1, %d;" ::: "memory");' % NT)
+        em("for (int t = 0; t < %d; ++t) {" % P)
+        em.ind += 1
+        em("const int s = r0 + t;")
+        em("if (s >= S) break;")
+        em("const int i = s / nkp, j = s - i * nkp;")
+        em("if (i != cur) {")
+        em.ind += 1
+        em("const double* __restrict__ bc = sbra + cur * %d;" % NB)
+        ff = 0
+        for ab in range(nab):
+            for k, h in enumerate(nz(fb[ab])):
+                e = offb[ab] + k
+                em("{ const double eb = bc[%d];" % (5 + e))
+                for cd in blk:
+                    em("  o%d_%d = fma(eb, g%d_%d, o%d_%d);" % (ab, cd, cd, hidx[h], ab, cd))
+                    ff += 2
+                em("}")
+        for cd in blk:
+            for h in Hb:
+                em("g%d_%d = 0.0;" % (cd, hidx[h]))
+        em("cur = i;")
+        em.ind -= 1
+        em("}")
+        em("const double* __restrict__ kj = kprim + j * %d;" % NK)
+        em("const double* __restrict__ src = sR + t * %d + lane;" % (NR * 32))
+        cons = {}
+        for cd in blk:
+            for k, (tau, nu, phi) in enumerate(nz(fk[cd])):
+                sg = -1 if (tau + nu + phi) % 2 else 1
+                em("const double ek%d_%d = %skj[%d];" % (cd, k, "-" if sg < 0 else "", 5 + offk[cd] + k))
+                for h in Hb:
+                    cons.setdefault((h[0] + tau, h[1] + nu, h[2] + phi), []).append((cd, k, h))
+        for key in need:
+            if key not in cons:
+                continue
+            em("{ const double r = src[%d];" % (32 * ridx[key]))
+            for (cd, k, h) in cons[key]:
+                em("  g%d_%d = fma(ek%d_%d, r, g%d_%d);" % (cd, hidx[h], cd, k, cd, hidx[h]))
+                pf += 2
+            em("}")
+        em.ind -= 1
+        em("}")
+        em('asm volatile("bar.sync 1, %d;" ::: "memory");' % NT)
+        em.ind -= 1
+        em("}")
+        em("if (S > 0) {")
+        em.ind += 1
+        em("const double* __restrict__ bc = sbra + cur * %d;" % NB)
+        for ab in range(nab):
+            for k, h in enumerate(nz(fb[ab])):
+                e = offb[ab] + k
+                em("{ const double eb = bc[%d];" % (5 + e))
+                for cd in blk:
+                    em("  o%d_%d = fma(eb, g%d_%d, o%d_%d);" % (ab, cd, cd, hidx[h], ab, cd))
+                em("}")
+        em.ind -= 1
+        em("}")
+        em("if (ok) {")
+        em.ind += 1
+        qf = emit_digest(em, spin, blk, nab, na, nb_, nd)
+        em.ind -= 1
+        em("}")
+        fl["flush"] += ff
+        fl["quartet"] += qf
+        em.ind -= 1
+        em("} break;")
+    em("}")
+    fl["prim"] = pf
+    em("{")
+    em("  const int fP = bp.fP, fQ = bp.fQ;")
+    em("  const double s2 = 2.0 * deg;")
+    for ab in range(nab):
+        aa, bb = divmod(ab, nb_)
+        em("  { const double v = sqb::warp_sum(s2 * jab%d); if (lane == 0 && v != 0.0) atomicAdd(a.Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
+    em("}")
+    em("sqb::count_add(a.counters + 0, (ok && wp == 0) ? 1ull : 0ull);")
+    em("sqb::count_add(a.counters + 1, nprimq);")
+    em("sqb::count_add(a.counters + 2, (ok && wp == 0) ? (unsigned long long)nbp : 0ull);")
+    em("sqb::count_add(a.counters + 3, (ok && wp == 0) ? 1ull : 0ull);")
+    out.extend(em.lines)
+    out.append("}")
+    return "\n".join(out) + "\n", {"name": name, "flops": fl, "P": P, "NR": NR}
 
 
 def write_if_changed(path, text):
@@ -412,6 +636,11 @@ def main():
         for spin in ("R", "U"):
             s, m = gen_class(bra, ket, spin)
             src.append(s)
+            m["ws"] = None
+            if USE_WS and ws_plan(bra, ket) is not None:
+                s2, m2 = gen_class_ws(bra, ket, spin)
+                src.append(s2)
+                m["ws"] = m2
             metas.append(m)
         fn = "jk_%s_%s.cu" % (bra, ket)
         write_if_changed(os.path.join(outdir, fn), "\n".join(src))
@@ -421,23 +650,33 @@ def main():
            '#include "../jk_registry.h"', '']
     for m in metas:
         reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["name"])
+        if m["ws"]:
+            reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["ws"]["name"])
     reg.append("")
     reg.append("namespace sqb {")
     reg.append("const char* const kPairClassNames[%d] = {%s};" % (len(PAIRS), ", ".join('"%s"' % p for p in PAIRS)))
     reg.append("const ClassKernel kClassKernels[%d] = {" % (len(metas) // 2))
     for i in range(0, len(metas), 2):
         r, u = metas[i], metas[i + 1]
-        reg.append('  {%d, %d, %d, %d, %d, %d, %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+        wr, wu = r["ws"], u["ws"]
+        reg.append('  {%d, %d, %d, %d, %d, %d, %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d,' % (
             PAIRS.index(r["bra"]), PAIRS.index(r["ket"]), r["nab"], r["ncd"], r["neb"], r["nek"],
             r["Lt"], r["flops"]["passes"], r["name"], u["name"], r["flops"]["prim"], r["flops"]["flush"],
             r["flops"]["quartet"]))
+        if wr:
+            reg.append('   %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+                wr["P"], wr["NR"], wr["name"], wu["name"], wr["flops"]["prim"], wr["flops"]["flush"],
+                wr["flops"]["quartet"]))
+        else:
+            reg.append('   0, 0, nullptr, nullptr, 0, 0, 0},')
     reg.append("};")
     reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
     reg.append("}  // namespace sqb")
     write_if_changed(os.path.join(outdir, "jk_registry.cu"), "\n".join(reg) + "\n")
     files.append("jk_registry.cu")
-    write_if_changed(os.path.join(outdir, "jk_flops.json"),
-                     json.dumps({m["name"]: m["flops"] for m in metas}, indent=0))
+    fj = {m["name"]: m["flops"] for m in metas}
+    fj.update({m["ws"]["name"]: m["ws"]["flops"] for m in metas if m["ws"]})
+    write_if_changed(os.path.join(outdir, "jk_flops.json"), json.dumps(fj, indent=0))
     write_if_changed(os.path.join(outdir, "files.txt"), "\n".join(files) + "\n")
     print("generated %d kernels in %d files" % (len(metas), len(files)))
 

@@ -207,6 +207,8 @@ struct sqb200_jk {
     int total = 0;
   };
   std::map<std::pair<double, double>, Work> work;
+  bool use_ws = true;           // warp-specialised form where a class has one (SQB200_WS=0 disables)
+  std::vector<char> ran_ws;     // per class kernel: which form the last build launched
   std::vector<long long> last_counts;
   long long last_flops = 0;
   int last_launches = 0;        // kernels enqueued by the last build
@@ -506,9 +508,11 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
         const int b0 = B.sub[sx], b1 = B.sub[sx + 1], k0s = T.sub[sy], k1s = T.sub[sy + 1];
         const int nbp = B.pairs[b0].nprim, nkp = T.pairs[k0s].nprim;
         // split the bra primitives over up to 32 threads when a quartet has many primitives
+        // (the warp-specialised form takes 32 kets per CTA, one lane each)
+        const bool ws = c->use_ws && K.ws_r != nullptr;
         int isplit = 1;
-        while (isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
-        const int kper = 128 / isplit;
+        while (!ws && isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
+        const int kper = ws ? 32 : 128 / isplit;
         for (int b = b0; b < b1; ++b) {
           const double sb = B.pairs[b].schwarz;
           if (!(sb > 0.0)) break;   // sorted: the rest are zero
@@ -571,8 +575,12 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
     a.cut_outer = outer; a.cut_fixed = fixed; a.dscreen_rmax = dscreen;
     const sqb::WorkItem* items = w->d_items + w->first[s];
     void* args[] = {&a, &items};
-    const size_t smem = (size_t)B.max_nprim * B.stride * sizeof(double);
-    const void* fn = uhf ? K.fn_u : K.fn_r;
+    const bool ws = c->use_ws && K.ws_r != nullptr;
+    c->ran_ws[w->kernel[s]] = ws;
+    const size_t smem = (size_t)B.max_nprim * B.stride * sizeof(double) +
+                        (ws ? (size_t)K.ws_warps * K.ws_nr * 32 * sizeof(double) : 0);
+    const void* fn = ws ? (uhf ? K.ws_u : K.ws_r) : (uhf ? K.fn_u : K.fn_r);
+    const dim3 grid(w->count[s], ws ? 1 : K.passes), block(ws ? 32 * K.ws_warps : 128);
     if (smem > 48 * 1024) CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     sqb200_jk::Ev ev{w->kernel[s], nullptr, nullptr};
     if (c->profile) {
@@ -580,7 +588,7 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
       CUDA_OK(cudaEventCreate(&ev.b));
       CUDA_OK(cudaEventRecord(ev.a, st));
     }
-    CUDA_OK(cudaLaunchKernel(fn, dim3(w->count[s], K.passes), dim3(128), args, smem, st));
+    CUDA_OK(cudaLaunchKernel(fn, grid, block, args, smem, st));
     if (c->profile) {
       CUDA_OK(cudaEventRecord(ev.b, st));
       c->events.push_back(ev);
@@ -609,6 +617,9 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   CUDA_OK(cudaSetDevice(device));
   sqb200_jk* c = new sqb200_jk();
   c->device = device;
+  const char* ws_env = getenv("SQB200_WS");
+  c->use_ws = !(ws_env && ws_env[0] == '0');
+  c->ran_ws.assign(sqb::kNumClassKernels, 0);
   c->nbf = nbf;
   int rc = build_shells(nbf, nprim, lmn, xyz, exps, ncoefs, c->shells);
   if (rc) { delete c; return rc; }
@@ -710,8 +721,10 @@ int sqb200_jk_stats(sqb200_jk* c, long long* out, int n) {
     const sqb::ClassKernel& K = sqb::kClassKernels[k];
     q += (long long)h[4 * k];
     pq += (long long)h[4 * k + 1];
-    fl += (long long)h[4 * k + 1] * K.flops_prim + (long long)h[4 * k + 2] * K.flops_flush +
-          (long long)h[4 * k + 3] * K.flops_quartet;
+    const bool ws = k < (int)c->ran_ws.size() && c->ran_ws[k];
+    fl += (long long)h[4 * k + 1] * (ws ? K.ws_flops_prim : K.flops_prim) +
+          (long long)h[4 * k + 2] * (ws ? K.ws_flops_flush : K.flops_flush) +
+          (long long)h[4 * k + 3] * (ws ? K.ws_flops_quartet : K.flops_quartet);
   }
   long long v[6] = {q, pq, fl, (long long)c->ns, 0, (long long)c->last_launches};
   for (int k = 0; k < sqb::kNumPairClasses; ++k) v[4] += (long long)c->cls[k].pairs.size();
@@ -764,7 +777,10 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
     row[0] = k;
     row[1] = (double)c->prof_launches[k];
     row[2] = c->prof_ms[k];
-    row[3] = (double)h[4 * k + 1] * K.flops_prim + (double)h[4 * k + 2] * K.flops_flush + (double)h[4 * k + 3] * K.flops_quartet;
+    const bool ws = c->ran_ws[k];
+    row[3] = (double)h[4 * k + 1] * (ws ? K.ws_flops_prim : K.flops_prim) +
+             (double)h[4 * k + 2] * (ws ? K.ws_flops_flush : K.flops_flush) +
+             (double)h[4 * k + 3] * (ws ? K.ws_flops_quartet : K.flops_quartet);
     row[4] = (double)h[4 * k + 1];
     row[5] = (double)h[4 * k];
     ++r;

@@ -18,6 +18,12 @@ struct ClassKernel {
   int flops_prim;         // FP64 ops per primitive quartet (all passes)
   int flops_flush;        // FP64 ops per bra primitive and ket pair (all passes)
   int flops_quartet;      // FP64 ops of one digestion (all passes) of a (partial) quartet block
+  // warp-specialised form (null when the class has one pass or its R buffer does not fit):
+  // one CTA of 32*ws_warps threads = all passes of 32 quartets, R staged in shared memory
+  int ws_warps, ws_nr;
+  const void* ws_r;
+  const void* ws_u;
+  int ws_flops_prim, ws_flops_flush, ws_flops_quartet;
 };
 
 extern const ClassKernel kClassKernels[];
