@@ -62,6 +62,26 @@ int sqb200_jk_build_device(sqb200_jk *ctx, const double *dPA, const double *dPB,
                            double dscreen_rmax, double *dJT, double *dKA, double *dKB,
                            void *stream);
 
+/* The device build of sqb200_jk_build_device for callers that must not allocate GPU memory:
+ * a program whose device memory is entirely owned by its own allocator (a framework's
+ * caching allocator that has reserved the GPU), or a latency-critical loop that cannot afford
+ * the implicit device-wide synchronisation of cudaMalloc/cudaFree.  No counterpart in the
+ * reference (an addition of this library).  This call allocates nothing: all its scratch
+ * (density sum, block maxima, J/K accumulators, counters, work list) lives in one static
+ * device array of about 3.5 MB that every GPU loading the library keeps until exit.
+ * Limits: nbf <= 256 and at most 65536 work items; larger inputs return SQB200_EINVAL with
+ * a message.  The context itself (sqb200_jk_create) must already exist.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  Every call shares the one
+ * array, so calls that overlap on the GPU (other streams, other threads, other contexts on
+ * the same device) race; serialise them.  Buffers are device pointers on the context's
+ * device, enqueued on `stream` (NULL = the context's stream); not synchronised.  Counters of
+ * sqb200_jk_stats are not updated by this call. */
+int sqb200_jk_build_noalloc(sqb200_jk *ctx, const double *dPA, const double *dPB,
+                            int restricted, double scf_cutoff, double fixed_cutoff,
+                            double dscreen_rmax, double *dJT, double *dKA, double *dKB,
+                            void *stream);
+
 /* Counters of the last build: out[0] shell quartets computed, out[1] primitive quartets
  * evaluated, out[2] algorithmic FP64 operations (per-class operation table),
  * out[3] shells, out[4] shell pairs, out[5] kernels the build enqueued.

@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -837,3 +838,147 @@ int sqb200_jk_mem_cutoff(sqb200_jk* c, double fixed, int max_mem_mb, double* out
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- build without allocation
+//
+// sqb200_jk_build_noalloc: the J/K build of sqb200_jk_build_device with every piece of scratch
+// (PT, PM, the J/K accumulators, the class counters and the work list) placed in one
+// file-scope device array instead of buffers the library allocates.  The array is sized for
+// at most kNoAllocMaxNbf basis functions and kNoAllocMaxItems work items; every device that
+// loads the library holds it until the process exits.
+
+namespace {
+
+constexpr int kNoAllocMaxNbf = 256;
+constexpr int kNoAllocMaxItems = 65536;
+constexpr int kNoAllocMaxKernels = 64;
+constexpr size_t kNoAllocMat = (size_t)kNoAllocMaxNbf * kNoAllocMaxNbf;          // doubles per matrix
+constexpr size_t kNoAllocCountersOff = 5 * kNoAllocMat * sizeof(double);            // PT PM J KA KB
+constexpr size_t kNoAllocItemsOff = kNoAllocCountersOff + 4 * kNoAllocMaxKernels * sizeof(unsigned long long);
+constexpr size_t kNoAllocBytes = kNoAllocItemsOff + (size_t)kNoAllocMaxItems * sizeof(sqb::WorkItem);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up once per device; the
+// host-side symbol itself is not a device address).
+int noalloc_scratch(int device, unsigned char** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (device < 0 || device >= 64) return fail(SQB200_EINVAL, "device index beyond 63");
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return fail(SQB200_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    g_noalloc_addr[device] = p;
+  }
+  *out = (unsigned char*)g_noalloc_addr[device];
+  return SQB200_OK;
+}
+
+// The work list of the standard kernel form on the host (no device copy kept).
+void noalloc_items(const sqb200_jk* c, double outer, double fixed, std::vector<sqb::WorkItem>& items,
+                   std::vector<int>& kernel, std::vector<int>& first, std::vector<int>& count) {
+  items.clear(); kernel.clear(); first.clear(); count.clear();
+  const double cut = std::max(outer, fixed);
+  for (int ki = 0; ki < sqb::kNumClassKernels; ++ki) {
+    const sqb::ClassKernel& K = sqb::kClassKernels[ki];
+    const PairClass& B = c->cls[K.bra_cls];
+    const PairClass& T = c->cls[K.ket_cls];
+    if (B.pairs.empty() || T.pairs.empty()) continue;
+    const int f0 = (int)items.size();
+    const bool same = K.bra_cls == K.ket_cls;
+    for (size_t sx = 0; sx + 1 < B.sub.size(); ++sx)
+      for (size_t sy = 0; sy + 1 < T.sub.size(); ++sy) {
+        if (same && sx > sy) continue;
+        const int b0 = B.sub[sx], b1 = B.sub[sx + 1], k0s = T.sub[sy], k1s = T.sub[sy + 1];
+        const int nbp = B.pairs[b0].nprim, nkp = T.pairs[k0s].nprim;
+        int isplit = 1;
+        while (isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
+        const int kper = 128 / isplit;
+        for (int b = b0; b < b1; ++b) {
+          const double sb = B.pairs[b].schwarz;
+          if (!(sb > 0.0)) break;
+          const double thr = cut / sb * (1.0 - 1e-12);
+          int lo = k0s, hi = k1s;
+          while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if (T.pairs[mid].schwarz >= thr) lo = mid + 1; else hi = mid;
+          }
+          const int start = (same && sx == sy) ? b : k0s;
+          for (int k0 = start; k0 < lo; k0 += kper) items.push_back({b, k0, std::min(kper, lo - k0), isplit});
+        }
+      }
+    if ((int)items.size() > f0) {
+      kernel.push_back(ki);
+      first.push_back(f0);
+      count.push_back((int)items.size() - f0);
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" int sqb200_jk_build_noalloc(sqb200_jk* c, const double* dPA, const double* dPB, int restricted,
+                                       double outer, double fixed, double dscreen, double* dJT, double* dKA,
+                                       double* dKB, void* stream) {
+  if (!c || !dPA || !dJT || !dKA) return fail(SQB200_EINVAL, "null argument");
+  if (!restricted && (dPB == nullptr || dKB == nullptr)) return fail(SQB200_EINVAL, "unrestricted build needs PB and KB");
+  if (c->nbf > kNoAllocMaxNbf)
+    return fail(SQB200_EINVAL, "sqb200_jk_build_noalloc: " + std::to_string(c->nbf) + " basis functions exceed its limit of " +
+                                   std::to_string(kNoAllocMaxNbf));
+  if (sqb::kNumClassKernels > kNoAllocMaxKernels) return fail(SQB200_EINVAL, "class table larger than the scratch counters");
+  CUDA_OK(cudaSetDevice(c->device));
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(c->device, &base);
+  if (rc) return rc;
+  thread_local std::vector<sqb::WorkItem> items;
+  thread_local std::vector<int> kernel, first, count;
+  noalloc_items(c, outer, fixed, items, kernel, first, count);
+  if ((int)items.size() > kNoAllocMaxItems)
+    return fail(SQB200_EINVAL, "sqb200_jk_build_noalloc: " + std::to_string(items.size()) +
+                                   " work items exceed its limit of " + std::to_string(kNoAllocMaxItems));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const int n = c->nbf, nn = n * n, uhf = restricted ? 0 : 1;
+  if (dPB == nullptr) dPB = dPA;
+  double* PT = (double*)base;
+  double* PM = PT + kNoAllocMat;
+  double* J = PM + kNoAllocMat;
+  double* KA = J + kNoAllocMat;
+  double* KB = KA + kNoAllocMat;
+  unsigned long long* counters = (unsigned long long*)(base + kNoAllocCountersOff);
+  sqb::WorkItem* d_items = (sqb::WorkItem*)(base + kNoAllocItemsOff);
+  if (!items.empty())
+    CUDA_OK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(sqb::WorkItem), cudaMemcpyHostToDevice, st));
+  // k_prep zeroes J, KA (and KB when unrestricted); the counters are cleared here
+  k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, PT, J, KA, KB, nn, uhf);
+  k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, PT, c->d_shfirst, c->d_shn, c->ns, n, PM);
+  CUDA_OK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 4 * sqb::kNumClassKernels, st));
+  for (size_t s = 0; s < kernel.size(); ++s) {
+    const sqb::ClassKernel& K = sqb::kClassKernels[kernel[s]];
+    const PairClass& B = c->cls[K.bra_cls];
+    const PairClass& T = c->cls[K.ket_cls];
+    sqb::JKArgs a;
+    memset(&a, 0, sizeof(a));
+    a.bra_pairs = B.d_pairs; a.bra_prims = B.d_prims;
+    a.ket_pairs = T.d_pairs; a.ket_prims = T.d_prims;
+    a.PA = dPA; a.PB = dPB; a.PT = PT; a.PM = PM;
+    a.Jacc = J; a.KAacc = KA; a.KBacc = KB;
+    a.boys_tab = c->d_boys;
+    a.counters = counters + 4 * kernel[s];
+    a.nbf = n; a.ns = c->ns;
+    a.same_class = K.bra_cls == K.ket_cls;
+    a.cut_outer = outer; a.cut_fixed = fixed; a.dscreen_rmax = dscreen;
+    const sqb::WorkItem* it = d_items + first[s];
+    void* args[] = {&a, &it};
+    const size_t smem = (size_t)B.max_nprim * B.stride * sizeof(double);
+    const void* fn = uhf ? K.fn_u : K.fn_r;
+    if (smem > 48 * 1024) CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_OK(cudaLaunchKernel(fn, dim3(count[s], K.passes), dim3(128), args, smem, st));
+  }
+  k_finalize<<<grid_for(nn, 256), 256, 0, st>>>(J, KA, KB, dJT, dKA, dKB, n, uhf);
+  CUDA_OK(cudaGetLastError());
+  return SQB200_OK;
+}
