@@ -98,8 +98,17 @@ int sqb200_jk_profile(sqb200_jk *ctx, int enable);
  * quartets of that launch, shell quartets of that launch]; *nrows receives the count. */
 int sqb200_jk_profile_read(sqb200_jk *ctx, double *rows, int max_rows, int *nrows);
 
-/* "bra|ket" pair-class name of a class-kernel index, e.g. "LL|LS". */
+/* "bra|ket" pair-class name of a class-kernel index, e.g. "LL|LS" ("LL|LS f32" for the
+ * mixed-precision form of that class). */
 const char *sqb200_jk_class_name(int k);
+
+/* Mixed precision: shell quartets whose Schwarz product Sch(PQ)*Sch(IJ) is below fp32_below
+ * evaluate their Hermite integrals and contractions in FP32 (setup, Boys function, screening
+ * and every J/K accumulation stay FP64); quartets above it, and the classes of highest angular
+ * momentum (total L >= 7), stay FP64.  0 (the default) = plain FP64.  Applies to the
+ * following builds of the context (not to sqb200_jk_build_noalloc).  No reference
+ * counterpart: the reference computes every quartet in FP64. */
+int sqb200_jk_set_precision(sqb200_jk *ctx, double fp32_below);
 
 /* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,
  * src/matrix.c:389-440), written to the host array S (nbf*nbf). */

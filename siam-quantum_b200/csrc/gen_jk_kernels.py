@@ -50,6 +50,7 @@ PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
 PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
 STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out accumulators per pass
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
+F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
 USE_WS = int(os.environ.get("SQB_WS", "0"))   # also emit warp-specialised multi-pass kernels (measured slower on B200; opt-in)
 CTA = 128
 
@@ -88,7 +89,7 @@ class Emitter:
         self.lines.append("  " * self.ind + s)
 
 
-def gen_R(em, L, need, cons=None, emit_use=None):
+def gen_R(em, L, need, cons=None, emit_use=None, rt="double", fma="fma"):
     """Emit R^{(0)}_{tuv} for (t,u,v) in need; returns flop count and name map.  When
     emit_use is given it is called right after each R^{(0)} value is produced, so its
     consumers follow it and the value dies early (lower register pressure)."""
@@ -116,13 +117,13 @@ def gen_R(em, L, need, cons=None, emit_use=None):
         if d - 1 > 0:
             l_ = get(*lo)
             if d - 1 == 1:
-                em("const double %s = fma(%s, %s, %s);" % (name, ax, h, l_))
+                em("const %s %s = %s(%s, %s, %s);" % (rt, name, fma, ax, h, l_))
                 flops[0] += 2
             else:
-                em("const double %s = fma(%s, %s, %d.0 * %s);" % (name, ax, h, d - 1, l_))
+                em("const %s %s = %s(%s, %s, %d.0%s * %s);" % (rt, name, fma, ax, h, d - 1, "f" if rt == "float" else "", l_))
                 flops[0] += 3
         else:
-            em("const double %s = %s * %s;" % (name, ax, h))
+            em("const %s %s = %s * %s;" % (rt, name, ax, h))
             flops[0] += 1
         have[key] = name
         return name
@@ -141,8 +142,14 @@ def boys_flops(M):
     return 8 * 3 + M * 3
 
 
-def gen_class(bra, ket, spin):
-    """Return (kernel source, metadata) for class (bra|ket) and spin 'R' or 'U'."""
+def gen_class(bra, ket, spin, prec="D"):
+    """Return (kernel source, metadata) for class (bra|ket) and spin 'R' or 'U'.  prec "F"
+    emits the mixed form: primitive setup, prefactor cut and Boys function in FP64, Hermite
+    integrals, E tables and contracted accumulators in FP32, digestion into the FP64 J/K
+    accumulators in FP64."""
+    F32 = prec == "F"
+    RT = "float" if F32 else "double"
+    FMA = "fmaf" if F32 else "fma"
     fb, offb, layb = etable(bra)
     fk, offk, layk = etable(ket)
     nab, ncd = len(fb), len(fk)
@@ -156,18 +163,22 @@ def gen_class(bra, ket, spin):
     NK = 5 + len(layk)
     per = max(1, STATE_MAX // (len(Hb) + nab))
     blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
-    name = "jk_%s_%s_%s" % (bra, ket, spin)
+    name = "jk_%s_%s_%s%s" % (bra, ket, spin, "_f32" if F32 else "")
     fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks)}
 
     em = Emitter()
     out = []
     out.append('extern "C" __global__ void __launch_bounds__(%d)' % CTA)
     out.append("%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name)
-    em("extern __shared__ double sbra[];")
+    if F32:
+        em("extern __shared__ float sbra_f32[];")
+        em("float* __restrict__ sbra = sbra_f32;")
+    else:
+        em("extern __shared__ double sbra[];")
     em("const sqb::WorkItem it = items[blockIdx.x];")
     em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
     em("const int N = a.nbf;")
-    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
+    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims%s[bp.poff + x];" % (NB, "_f" if F32 else ""))
     em("__syncthreads();")
     em("const int isplit = it.isplit;                 // threads sharing one quartet (bra primitives split)")
     em("const int kl = threadIdx.x / isplit, grp = threadIdx.x - kl * isplit;")
@@ -195,7 +206,7 @@ def gen_class(bra, ket, spin):
     em("unsigned long long nprimq = 0, nflush = 0;")
     em("if (ok) {")
     em.ind += 1
-    em("const double* __restrict__ kprim = a.ket_prims + kp.poff;")
+    em("const %s* __restrict__ kprim = a.ket_prims%s + kp.poff;" % (RT, "_f" if F32 else ""))
     em("const int nbp = bp.nprim, nkp = kp.nprim;")
     em("nflush = pass == 0 ? (unsigned long long)((nbp - grp + isplit - 1) / isplit) : 0ull;")
     em("const double* __restrict__ PA = a.PA;")
@@ -208,14 +219,14 @@ def gen_class(bra, ket, spin):
         em.ind += 1
         for ab in range(nab):
             for cd in blk:
-                em("double o%d_%d = 0.0;" % (ab, cd))
+                em("%s o%d_%d = 0;" % (RT, ab, cd))
         em("for (int i = grp; i < nbp; i += isplit) {")
         em.ind += 1
-        em("const double* __restrict__ bi = sbra + i * %d;" % NB)
+        em("const %s* __restrict__ bi = sbra + i * %d;" % (RT, NB))
         em("const double p = bi[0], Px = bi[1], Py = bi[2], Pz = bi[3], kpb = bi[4];")
         for cd in blk:
             for h in Hb:
-                em("double g%d_%d = 0.0;" % (cd, hidx[h]))
+                em("%s g%d_%d = 0;" % (RT, cd, hidx[h]))
         # ket E-table entries this block reads
         kent = []
         for cd in blk:
@@ -246,7 +257,7 @@ def gen_class(bra, ket, spin):
             em("const double rs = rsqrt(pq);")
             em("if (TWO_PI_2_5 * kpb * kq * rs < PRIM_CUTOFF) continue;")
         else:
-            em("const double* __restrict__ kj = kprim + j * %d;" % NK)
+            em("const %s* __restrict__ kj = kprim + j * %d;" % (RT, NK))
             em("const double q = kj[0];")
             em("const double pq = p + q;")
             em("const double rs = rsqrt(pq);")
@@ -275,12 +286,12 @@ def gen_class(bra, ket, spin):
             if n > 0:
                 em("w *= m2a;")
                 pf += 1
-            em("const double b%d = w * F[%d];" % (n, n))
+            em("const %s b%d = %s(w * F[%d]);" % (RT, n, "(float)" if F32 else "", n))
             pf += 1
         # ket E coefficients of this block, signed by (-1)^(tau+nu+phi)
         if not PREFETCH:
             for (cd, k, e, sg) in kent:
-                em("const double ek%d_%d = %skj[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
+                em("const %s ek%d_%d = %skj[%d];" % (RT, cd, k, "-" if sg < 0 else "", 5 + e))
         # consumers of each R value: (cd, k, h) with h + (tau nu phi) = R index
         cons = {}
         for cd in blk:
@@ -288,8 +299,8 @@ def gen_class(bra, ket, spin):
                 for h in Hb:
                     cons.setdefault((h[0] + tau, h[1] + nu, h[2] + phi), []).append((cd, k, h))
         rn, rf = gen_R(em, Lp, need, cons=cons, emit_use=lambda key, name: [
-            (em("g%d_%d = fma(ek%d_%d, %s, g%d_%d);" % (cd, hidx[h], cd, k, name, cd, hidx[h])))
-            for (cd, k, h) in cons.get(key, [])])
+            (em("g%d_%d = %s(ek%d_%d, %s, g%d_%d);" % (cd, hidx[h], FMA, cd, k, name, cd, hidx[h])))
+            for (cd, k, h) in cons.get(key, [])], rt=RT, fma=FMA)
         pf += rf + 2 * sum(len(v) for v in cons.values())
         em.ind -= 1
         em("}")
@@ -298,9 +309,9 @@ def gen_class(bra, ket, spin):
         for ab in range(nab):
             for k, h in enumerate(nz(fb[ab])):
                 e = offb[ab] + k
-                em("{ const double eb = bi[%d];" % (5 + e))
+                em("{ const %s eb = bi[%d];" % (RT, 5 + e))
                 for cd in blk:
-                    em("  o%d_%d = fma(eb, g%d_%d, o%d_%d);" % (ab, cd, cd, hidx[h], ab, cd))
+                    em("  o%d_%d = %s(eb, g%d_%d, o%d_%d);" % (ab, cd, FMA, cd, hidx[h], ab, cd))
                     ff += 2
                 em("}")
         em.ind -= 1
@@ -641,6 +652,11 @@ def main():
                 s2, m2 = gen_class_ws(bra, ket, spin)
                 src.append(s2)
                 m["ws"] = m2
+            m["f32"] = None
+            if pair_L(bra) + pair_L(ket) <= F32_MAX_L:
+                s3, m3 = gen_class(bra, ket, spin, "F")
+                src.append(s3)
+                m["f32"] = m3
             metas.append(m)
         fn = "jk_%s_%s.cu" % (bra, ket)
         write_if_changed(os.path.join(outdir, fn), "\n".join(src))
@@ -652,6 +668,8 @@ def main():
         reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["name"])
         if m["ws"]:
             reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["ws"]["name"])
+        if m["f32"]:
+            reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["f32"]["name"])
     reg.append("")
     reg.append("namespace sqb {")
     reg.append("const char* const kPairClassNames[%d] = {%s};" % (len(PAIRS), ", ".join('"%s"' % p for p in PAIRS)))
@@ -664,11 +682,18 @@ def main():
             r["Lt"], r["flops"]["passes"], r["name"], u["name"], r["flops"]["prim"], r["flops"]["flush"],
             r["flops"]["quartet"]))
         if wr:
-            reg.append('   %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+            reg.append('   %d, %d, (const void*)%s, (const void*)%s, %d, %d, %d,' % (
                 wr["P"], wr["NR"], wr["name"], wu["name"], wr["flops"]["prim"], wr["flops"]["flush"],
                 wr["flops"]["quartet"]))
         else:
-            reg.append('   0, 0, nullptr, nullptr, 0, 0, 0},')
+            reg.append('   0, 0, nullptr, nullptr, 0, 0, 0,')
+        fr, fu = r["f32"], u["f32"]
+        if fr:
+            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+                fr["flops"]["passes"], fr["name"], fu["name"], fr["flops"]["prim"], fr["flops"]["flush"],
+                fr["flops"]["quartet"]))
+        else:
+            reg.append('   0, nullptr, nullptr, 0, 0, 0},')
     reg.append("};")
     reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
     reg.append("}  // namespace sqb")
@@ -676,6 +701,7 @@ def main():
     files.append("jk_registry.cu")
     fj = {m["name"]: m["flops"] for m in metas}
     fj.update({m["ws"]["name"]: m["ws"]["flops"] for m in metas if m["ws"]})
+    fj.update({m["f32"]["name"]: m["f32"]["flops"] for m in metas if m["f32"]})
     write_if_changed(os.path.join(outdir, "jk_flops.json"), json.dumps(fj, indent=0))
     write_if_changed(os.path.join(outdir, "files.txt"), "\n".join(files) + "\n")
     print("generated %d kernels in %d files" % (len(metas), len(files)))

@@ -58,6 +58,8 @@ struct JKArgs {
   int same_class;              // bra and ket pairs come from one class (pair identity possible)
   int pad;
   double cut_outer, cut_fixed, dscreen_rmax;
+  const float* bra_prims_f;    // FP32 copies of the primitive records (mixed-precision kernels)
+  const float* ket_prims_f;
 };
 
 // F_0..F_M at T.  M is a compile-time order so the recursion unrolls.

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -182,6 +183,7 @@ struct PairClass {
   std::vector<double> prims;
   sqb::PairRec* d_pairs = nullptr;
   double* d_prims = nullptr;
+  float* d_primsf = nullptr;     // FP32 copy for the mixed-precision kernels
 };
 
 }  // namespace
@@ -201,13 +203,16 @@ struct sqb200_jk {
   double *d_JT = nullptr, *d_KAo = nullptr, *d_KBo = nullptr;   // outputs for host builds
   unsigned long long* d_counters = nullptr;  // 3 per class kernel
   // work lists cached per (outer, fixed) cutoff
+  // a segment's kernel index v < K is the FP64 form of class v, v >= K the FP32 form of
+  // class v - K (K = kNumClassKernels); counters and timings use the same index
   struct Work {
-    std::vector<int> kernel;      // class-kernel index per segment
+    std::vector<int> kernel;      // kernel index per segment
     std::vector<int> first, count;
     sqb::WorkItem* d_items = nullptr;
     int total = 0;
   };
-  std::map<std::pair<double, double>, Work> work;
+  std::map<std::tuple<double, double, double>, Work> work;
+  double fp32_below = 0.0;      // quartets with Schwarz product below this use the FP32 form
   bool use_ws = true;           // warp-specialised form where a class has one (SQB200_WS=0 disables)
   std::vector<char> ran_ws;     // per class kernel: which form the last build launched
   std::vector<long long> last_counts;
@@ -464,6 +469,10 @@ int compute_schwarz_device(sqb200_jk* c, double* S_host) {
 
 void free_pairs(sqb200_jk* c) {
   for (int k = 0; k < sqb::kNumPairClasses; ++k) {
+    cudaFree(c->cls[k].d_primsf);
+    c->cls[k].d_primsf = nullptr;
+  }
+  for (int k = 0; k < sqb::kNumPairClasses; ++k) {
     cudaFree(c->cls[k].d_pairs);
     cudaFree(c->cls[k].d_prims);
     c->cls[k].d_pairs = nullptr;
@@ -479,20 +488,23 @@ int upload_pairs(sqb200_jk* c) {
     CUDA_OK(cudaMalloc(&pc.d_prims, pc.prims.size() * sizeof(double)));
     CUDA_OK(cudaMemcpy(pc.d_pairs, pc.pairs.data(), pc.pairs.size() * sizeof(sqb::PairRec), cudaMemcpyHostToDevice));
     CUDA_OK(cudaMemcpy(pc.d_prims, pc.prims.data(), pc.prims.size() * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<float> pf(pc.prims.begin(), pc.prims.end());
+    CUDA_OK(cudaMalloc(&pc.d_primsf, pf.size() * sizeof(float)));
+    CUDA_OK(cudaMemcpy(pc.d_primsf, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice));
   }
   return SQB200_OK;
 }
 
 // Work list: per class kernel, one item per (bra pair, <=128 ket pairs).
 int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) {
-  auto key = std::make_pair(outer, fixed);
+  auto key = std::make_tuple(outer, fixed, c->fp32_below);
   auto it = c->work.find(key);
   if (it != c->work.end()) {
     *out = &it->second;
     return SQB200_OK;
   }
   sqb200_jk::Work w;
-  std::vector<sqb::WorkItem> items;
+  std::vector<sqb::WorkItem> items, items32;
   const double cut = std::max(outer, fixed);
   for (int ki = 0; ki < sqb::kNumClassKernels; ++ki) {
     const sqb::ClassKernel& K = sqb::kClassKernels[ki];
@@ -501,6 +513,8 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
     if (B.pairs.empty() || T.pairs.empty()) continue;
     const int first = (int)items.size();
     const bool same = K.bra_cls == K.ket_cls;
+    const bool mixed = c->fp32_below > 0.0 && K.fn_r32 != nullptr;
+    items32.clear();
     // every (bra sub-list, ket sub-list) combination; inside one class each unordered pair of
     // sub-lists once, and inside one sub-list each unordered pair of pairs once (k >= b)
     for (size_t sx = 0; sx + 1 < B.sub.size(); ++sx)
@@ -526,7 +540,20 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
           }
           const int end = lo;
           const int start = (same && sx == sy) ? b : k0s;
-          for (int k0 = start; k0 < end; k0 += kper) items.push_back({b, k0, std::min(kper, end - k0), isplit});
+          // kets with Sch(bra)*Sch(ket) >= fp32_below (a prefix) stay FP64, the rest go FP32
+          int mid = end;
+          if (mixed) {
+            const double t32 = c->fp32_below / sb;
+            int l2 = start, h2 = end;
+            while (l2 < h2) {
+              const int m2 = (l2 + h2) / 2;
+              if (T.pairs[m2].schwarz >= t32) l2 = m2 + 1; else h2 = m2;
+            }
+            mid = l2;
+          }
+          for (int k0 = start; k0 < mid; k0 += kper) items.push_back({b, k0, std::min(kper, mid - k0), isplit});
+          for (int k0 = std::max(start, mid); k0 < end; k0 += kper)
+            items32.push_back({b, k0, std::min(kper, end - k0), isplit});
         }
       }
     const int cnt = (int)items.size() - first;
@@ -534,6 +561,12 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
       w.kernel.push_back(ki);
       w.first.push_back(first);
       w.count.push_back(cnt);
+    }
+    if (!items32.empty()) {
+      w.kernel.push_back(ki + sqb::kNumClassKernels);
+      w.first.push_back((int)items.size());
+      w.count.push_back((int)items32.size());
+      items.insert(items.end(), items32.begin(), items32.end());
     }
   }
   w.total = (int)items.size();
@@ -557,10 +590,13 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   if (rc) return rc;
   k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf);
   k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM);
-  CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 4 * sqb::kNumClassKernels, st));
+  CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 8 * sqb::kNumClassKernels, st));
   c->last_launches = 3 + (int)w->kernel.size();
   for (size_t s = 0; s < w->kernel.size(); ++s) {
-    const sqb::ClassKernel& K = sqb::kClassKernels[w->kernel[s]];
+    const int v = w->kernel[s];
+    const bool f32 = v >= sqb::kNumClassKernels;
+    const int kidx = f32 ? v - sqb::kNumClassKernels : v;
+    const sqb::ClassKernel& K = sqb::kClassKernels[kidx];
     const PairClass& B = c->cls[K.bra_cls];
     const PairClass& T = c->cls[K.ket_cls];
     sqb::JKArgs a;
@@ -570,20 +606,21 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
     a.PA = dPA; a.PB = dPB; a.PT = c->d_PT; a.PM = c->d_PM;
     a.Jacc = c->d_J; a.KAacc = c->d_KA; a.KBacc = c->d_KB;
     a.boys_tab = c->d_boys;
-    a.counters = c->d_counters + 4 * w->kernel[s];
+    a.counters = c->d_counters + 4 * v;
+    a.bra_prims_f = B.d_primsf; a.ket_prims_f = T.d_primsf;
     a.nbf = n; a.ns = c->ns;
     a.same_class = K.bra_cls == K.ket_cls;
     a.cut_outer = outer; a.cut_fixed = fixed; a.dscreen_rmax = dscreen;
     const sqb::WorkItem* items = w->d_items + w->first[s];
     void* args[] = {&a, &items};
-    const bool ws = c->use_ws && K.ws_r != nullptr;
-    c->ran_ws[w->kernel[s]] = ws;
-    const size_t smem = (size_t)B.max_nprim * B.stride * sizeof(double) +
+    const bool ws = !f32 && c->use_ws && K.ws_r != nullptr;
+    if (!f32) c->ran_ws[kidx] = ws;
+    const size_t smem = (size_t)B.max_nprim * B.stride * (f32 ? sizeof(float) : sizeof(double)) +
                         (ws ? (size_t)K.ws_warps * K.ws_nr * 32 * sizeof(double) : 0);
-    const void* fn = ws ? (uhf ? K.ws_u : K.ws_r) : (uhf ? K.fn_u : K.fn_r);
-    const dim3 grid(w->count[s], ws ? 1 : K.passes), block(ws ? 32 * K.ws_warps : 128);
+    const void* fn = f32 ? (uhf ? K.fn_u32 : K.fn_r32) : ws ? (uhf ? K.ws_u : K.ws_r) : (uhf ? K.fn_u : K.fn_r);
+    const dim3 grid(w->count[s], ws ? 1 : (f32 ? K.passes32 : K.passes)), block(ws ? 32 * K.ws_warps : 128);
     if (smem > 48 * 1024) CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    sqb200_jk::Ev ev{w->kernel[s], nullptr, nullptr};
+    sqb200_jk::Ev ev{v, nullptr, nullptr};
     if (c->profile) {
       CUDA_OK(cudaEventCreate(&ev.a));
       CUDA_OK(cudaEventCreate(&ev.b));
@@ -598,6 +635,19 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   k_finalize<<<grid_for(nn, 256), 256, 0, st>>>(c->d_J, c->d_KA, c->d_KB, dJT, dKA, dKB, n, uhf);
   CUDA_OK(cudaGetLastError());
   return SQB200_OK;
+}
+
+// Algorithmic FP64/FP32 operations of kernel index v (FP64 form v < K, FP32 form v - K)
+// from its four counters [quartets, primitive quartets, bra flushes, digestions].
+double kernel_flops(const sqb200_jk* c, int v, const unsigned long long* h) {
+  const int K_ = sqb::kNumClassKernels;
+  const bool f32 = v >= K_;
+  const sqb::ClassKernel& K = sqb::kClassKernels[f32 ? v - K_ : v];
+  const bool ws = !f32 && v < (int)c->ran_ws.size() && c->ran_ws[v];
+  const double fp = f32 ? K.f32_flops_prim : ws ? K.ws_flops_prim : K.flops_prim;
+  const double ff = f32 ? K.f32_flops_flush : ws ? K.ws_flops_flush : K.flops_flush;
+  const double fq = f32 ? K.f32_flops_quartet : ws ? K.ws_flops_quartet : K.flops_quartet;
+  return (double)h[1] * fp + (double)h[2] * ff + (double)h[3] * fq;
 }
 
 }  // namespace
@@ -648,7 +698,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   ALLOC(c->d_JT, nn * sizeof(double));
   ALLOC(c->d_KAo, nn * sizeof(double));
   ALLOC(c->d_KBo, nn * sizeof(double));
-  ALLOC(c->d_counters, 4 * sqb::kNumClassKernels * sizeof(unsigned long long));
+  ALLOC(c->d_counters, 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
 #undef ALLOC
   cudaError_t e = cudaMemcpy(c->d_boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_shfirst, fst.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
@@ -715,17 +765,13 @@ int sqb200_jk_stats(sqb200_jk* c, long long* out, int n) {
   if (!c || !out) return fail(SQB200_EINVAL, "null argument");
   CUDA_OK(cudaSetDevice(c->device));
   CUDA_OK(cudaStreamSynchronize(c->stream));
-  std::vector<unsigned long long> h(4 * sqb::kNumClassKernels);
+  std::vector<unsigned long long> h(8 * sqb::kNumClassKernels);
   CUDA_OK(cudaMemcpy(h.data(), c->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   long long q = 0, pq = 0, fl = 0;
-  for (int k = 0; k < sqb::kNumClassKernels; ++k) {
-    const sqb::ClassKernel& K = sqb::kClassKernels[k];
-    q += (long long)h[4 * k];
-    pq += (long long)h[4 * k + 1];
-    const bool ws = k < (int)c->ran_ws.size() && c->ran_ws[k];
-    fl += (long long)h[4 * k + 1] * (ws ? K.ws_flops_prim : K.flops_prim) +
-          (long long)h[4 * k + 2] * (ws ? K.ws_flops_flush : K.flops_flush) +
-          (long long)h[4 * k + 3] * (ws ? K.ws_flops_quartet : K.flops_quartet);
+  for (int v = 0; v < 2 * sqb::kNumClassKernels; ++v) {
+    q += (long long)h[4 * v];
+    pq += (long long)h[4 * v + 1];
+    fl += (long long)kernel_flops(c, v, &h[4 * v]);
   }
   long long v[6] = {q, pq, fl, (long long)c->ns, 0, (long long)c->last_launches};
   for (int k = 0; k < sqb::kNumPairClasses; ++k) v[4] += (long long)c->cls[k].pairs.size();
@@ -745,8 +791,8 @@ int sqb200_jk_profile(sqb200_jk* c, int enable) {
   CUDA_OK(cudaStreamSynchronize(c->stream));
   for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   c->events.clear();
-  c->prof_ms.assign(sqb::kNumClassKernels, 0.0);
-  c->prof_launches.assign(sqb::kNumClassKernels, 0);
+  c->prof_ms.assign(2 * sqb::kNumClassKernels, 0.0);
+  c->prof_launches.assign(2 * sqb::kNumClassKernels, 0);
   c->profile = enable != 0;
   return SQB200_OK;
 }
@@ -758,9 +804,9 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
     CUDA_OK(cudaEventSynchronize(e.b));
     float ms = 0.f;
     CUDA_OK(cudaEventElapsedTime(&ms, e.a, e.b));
-    if (c->prof_ms.size() != (size_t)sqb::kNumClassKernels) {
-      c->prof_ms.assign(sqb::kNumClassKernels, 0.0);
-      c->prof_launches.assign(sqb::kNumClassKernels, 0);
+    if (c->prof_ms.size() != (size_t)(2 * sqb::kNumClassKernels)) {
+      c->prof_ms.assign(2 * sqb::kNumClassKernels, 0.0);
+      c->prof_launches.assign(2 * sqb::kNumClassKernels, 0);
     }
     c->prof_ms[e.kernel] += ms;
     c->prof_launches[e.kernel] += 1;
@@ -768,22 +814,18 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
     cudaEventDestroy(e.b);
   }
   c->events.clear();
-  std::vector<unsigned long long> h(4 * sqb::kNumClassKernels);
+  std::vector<unsigned long long> h(8 * sqb::kNumClassKernels);
   CUDA_OK(cudaMemcpy(h.data(), c->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   int r = 0;
-  for (int k = 0; k < sqb::kNumClassKernels && r < max_rows; ++k) {
-    if (c->prof_launches.empty() || c->prof_launches[k] == 0) continue;
-    const sqb::ClassKernel& K = sqb::kClassKernels[k];
+  for (int v = 0; v < 2 * sqb::kNumClassKernels && r < max_rows; ++v) {
+    if (c->prof_launches.empty() || c->prof_launches[v] == 0) continue;
     double* row = rows + 6 * r;
-    row[0] = k;
-    row[1] = (double)c->prof_launches[k];
-    row[2] = c->prof_ms[k];
-    const bool ws = c->ran_ws[k];
-    row[3] = (double)h[4 * k + 1] * (ws ? K.ws_flops_prim : K.flops_prim) +
-             (double)h[4 * k + 2] * (ws ? K.ws_flops_flush : K.flops_flush) +
-             (double)h[4 * k + 3] * (ws ? K.ws_flops_quartet : K.flops_quartet);
-    row[4] = (double)h[4 * k + 1];
-    row[5] = (double)h[4 * k];
+    row[0] = v;
+    row[1] = (double)c->prof_launches[v];
+    row[2] = c->prof_ms[v];
+    row[3] = kernel_flops(c, v, &h[4 * v]);
+    row[4] = (double)h[4 * v + 1];
+    row[5] = (double)h[4 * v];
     ++r;
   }
   *nrows = r;
@@ -791,13 +833,23 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
 }
 
 const char* sqb200_jk_class_name(int k) {
-  if (k < 0 || k >= sqb::kNumClassKernels) return "";
+  if (k < 0 || k >= 2 * sqb::kNumClassKernels) return "";
   static std::vector<std::string> names;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
   if (names.empty())
-    for (int i = 0; i < sqb::kNumClassKernels; ++i)
-      names.push_back(std::string(sqb::kPairClassNames[sqb::kClassKernels[i].bra_cls]) + "|" +
-                      sqb::kPairClassNames[sqb::kClassKernels[i].ket_cls]);
+    for (int i = 0; i < 2 * sqb::kNumClassKernels; ++i) {
+      const sqb::ClassKernel& K = sqb::kClassKernels[i % sqb::kNumClassKernels];
+      names.push_back(std::string(sqb::kPairClassNames[K.bra_cls]) + "|" + sqb::kPairClassNames[K.ket_cls] +
+                      (i >= sqb::kNumClassKernels ? " f32" : ""));
+    }
   return names[k].c_str();
+}
+
+int sqb200_jk_set_precision(sqb200_jk* c, double fp32_below) {
+  if (!c || !(fp32_below >= 0.0)) return fail(SQB200_EINVAL, "null context or negative threshold");
+  c->fp32_below = fp32_below;
+  return SQB200_OK;
 }
 
 int sqb200_jk_mem_cutoff(sqb200_jk* c, double fixed, int max_mem_mb, double* out) {

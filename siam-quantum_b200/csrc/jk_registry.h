@@ -24,6 +24,12 @@ struct ClassKernel {
   const void* ws_r;
   const void* ws_u;
   int ws_flops_prim, ws_flops_flush, ws_flops_quartet;
+  // mixed form (FP32 Hermite integrals and contraction, FP64 Boys/setup/accumulation); null
+  // for the classes of highest angular momentum, whose small quartets stay in FP64
+  int passes32;
+  const void* fn_r32;
+  const void* fn_u32;
+  int f32_flops_prim, f32_flops_flush, f32_flops_quartet;
 };
 
 extern const ClassKernel kClassKernels[];

@@ -22,7 +22,9 @@
  * Differences: quartets are evaluated exactly (McMurchie-Davidson in FP64); the reference's
  * monopole approximation for uncached quartets on later visits (src/matrix.c:3945-3949) is not
  * used.  Errors print a message and exit(-1), as the reference does.
- * Environment: SQB200_DEVICE selects the CUDA device (default 0).
+ * Environment: SQB200_DEVICE selects the CUDA device (default 0); SQB200_FP32_BELOW=<tau>
+ * evaluates quartets whose Schwarz product is below tau in FP32 (mixed precision; the
+ * reference's SCF passes difference densities, so these errors shrink as SCF converges).
  */
 #include <math.h>
 #include <stdio.h>
@@ -65,6 +67,8 @@ static void create_context(int nBasis, const struct GTOBasis_t *gto, const doubl
 	int rc = sqb200_jk_create(&g_ctx, nBasis, nprim, lmn, xyz, ex, nc, schwarz, dev ? atoi(dev) : 0);
 	free(nprim); free(lmn); free(xyz); free(ex); free(nc);
 	if (rc) die("sqb200_jk_create", rc);
+	const char *f32 = getenv("SQB200_FP32_BELOW");
+	if (f32 && (rc = sqb200_jk_set_precision(g_ctx, atof(f32)))) die("sqb200_jk_set_precision", rc);
 }
 
 void GTO_JK_Matrix_Quartet_Parallel(

@@ -22,7 +22,8 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
 EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_jk_build_device",
            "sqb200_jk_stats", "sqb200_jk_profile", "sqb200_jk_profile_read", "sqb200_jk_class_name",
-           "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_peak_fma", "sqb200_last_error"]
+           "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_jk_set_precision", "sqb200_peak_fma",
+           "sqb200_last_error"]
 
 
 class SQB200Error(RuntimeError):
@@ -51,6 +52,7 @@ def load_library(path=LIB_PATH):
     L.sqb200_jk_profile.argtypes = [vp, ctypes.c_int]
     L.sqb200_jk_profile_read.argtypes = [vp, _f64p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.sqb200_jk_class_name.argtypes = [ctypes.c_int]
+    L.sqb200_jk_set_precision.argtypes = [vp, ctypes.c_double]
     L.sqb200_peak_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:
@@ -139,6 +141,10 @@ class JKEngine:
                         "ms": float(r[2]), "flops": float(r[3]), "prim_quartets": int(r[4]),
                         "quartets": int(r[5])})
         return out
+
+    def set_precision(self, fp32_below):
+        """Quartets with Schwarz product below fp32_below use the FP32 kernel form (0 = FP64)."""
+        _check(_lib.sqb200_jk_set_precision(self._ctx, float(fp32_below)))
 
     def mem_cutoff(self, fixed_cutoff, max_mem_mb):
         v = ctypes.c_double()
