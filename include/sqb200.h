@@ -110,6 +110,13 @@ const char *sqb200_jk_class_name(int k);
  * counterpart: the reference computes every quartet in FP64. */
 int sqb200_jk_set_precision(sqb200_jk *ctx, double fp32_below);
 
+/* One-electron integrals of the context's basis on its device: overlap S, kinetic T and
+ * nuclear attraction V = -sum_C Z_C <p|1/|r-C||q> for natom point charges Z at axyz (bohr),
+ * each written to a host nbf*nbf array (the matrices the reference's uhf() builds with
+ * overlap/kinetic/nai, src/uhf.c:1307-1334; H = T + V). */
+int sqb200_oneint(sqb200_jk *ctx, int natom, const double *Z, const double *axyz,
+                  double *S, double *T, double *V);
+
 /* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,
  * src/matrix.c:389-440), written to the host array S (nbf*nbf). */
 int sqb200_jk_schwarz(sqb200_jk *ctx, double *S);

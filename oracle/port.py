@@ -144,3 +144,12 @@ def ref_schwarz(xyz_path, basis_path, n):
         out = os.path.join(d, "s.bin")
         ref_run(["schwarz", xyz_path, basis_path, out])
         return np.fromfile(out, dtype=np.float64).reshape(n, n)
+
+
+def ref_oneint(xyz_path, basis_path, n):
+    """S, T, V of the reference's uhf() set-up (GTO_overlap/GTO_kinetic/GTO_nuclei)."""
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "stv.bin")
+        ref_run(["oneint", xyz_path, basis_path, out])
+        m = np.fromfile(out, dtype=np.float64).reshape(3, n, n)
+        return m[0], m[1], m[2]

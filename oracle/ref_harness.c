@@ -17,6 +17,9 @@
  *   sqref scf     <xyz> <basis> <densout|-> [reference options...]
  *                 uhf() (src/uhf.c:1171) as sq.c:152-415 drives it; prints the total energy
  *                 with 12 decimals on stderr and writes PA,PB of the final orbitals
+ *   sqref oneint  <xyz> <basis> <out>
+ *                 S, T, V as uhf() builds them (src/uhf.c:1307-1334: GTO_overlap,
+ *                 GTO_kinetic, GTO_nuclei); writes S,T,V (3*n*n doubles)
  *   sqref bench   <xyz> <basis> <PA> <cutoff> <maxMem> <seconds>
  *                 repeated fresh restricted J/K builds for at least <seconds>; prints count
  */
@@ -167,6 +170,22 @@ int main(int argc, char **argv){
 			double *out[2] = {PA, PB};
 			write_mats(argv[4], n, 2, out);
 		}
+		return 0;
+	}
+
+	if(!strcmp(cmd, "oneint") && argc >= 5){
+		struct Molecule_t *mol;
+		struct GTOBasis_t *g = load_basis(argv[2], argv[3], &n, &mol);
+		double *S = calloc((size_t)n * n, 8), *T = calloc((size_t)n * n, 8),
+		       *V = calloc((size_t)n * n, 8);
+		for(int i = 0; i < n; i++)
+		for(int j = 0; j <= i; j++){
+			S[i * n + j] = S[j * n + i] = GTO_overlap(i, j, g);
+			T[i * n + j] = T[j * n + i] = GTO_kinetic(i, j, g);
+			V[i * n + j] = V[j * n + i] = GTO_nuclei(i, j, g, mol);
+		}
+		double *out[3] = {S, T, V};
+		write_mats(argv[4], n, 3, out);
 		return 0;
 	}
 

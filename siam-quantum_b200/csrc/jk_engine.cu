@@ -355,6 +355,111 @@ __global__ void k_schwarz(const sqb::PairRec* __restrict__ pairs, const double* 
   S[(size_t)(rec.fQ + b) * nbf + rec.fP + a] = v;
 }
 
+
+// ---------------------------------------------------------------- one-electron integrals
+//
+// Overlap S, kinetic T and nuclear attraction V over contracted Cartesian functions (the
+// reference builds them with overlap/kinetic/nai, src/int.c, for uhf(), src/uhf.c:1307-1334).
+// One thread per function pair (p, q), McMurchie-Davidson per primitive pair:
+//   S = c K (pi/p)^{3/2} Ex0 Ey0 Ez0,  with E^{ij}_0 the 1-D Hermite coefficients
+//   T = -1/2 sum_axes [ j(j-1) S(i,j-2) - 2b(2j+1) S(i,j) + 4b^2 S(i,j+2) ] x (other axes' S)
+//   V = -sum_C Z_C 2pi/p c K sum_tuv E_t E_u E_v R_tuv(p, P - C)
+
+__device__ void oe_hermite(double p, double xpa, double xpb, int la, int lb, double E[3][5][7]) {
+  const double h = 0.5 / p;
+  for (int i = 0; i <= la; ++i)
+    for (int j = 0; j <= lb; ++j)
+      for (int t = 0; t <= i + j; ++t) {
+        double v;
+        if (i == 0 && j == 0) v = (t == 0) ? 1.0 : 0.0;
+        else if (i > 0) {
+          v = xpa * E[i - 1][j][t];
+          if (t > 0) v += h * E[i - 1][j][t - 1];
+          if (t + 1 <= i - 1 + j) v += (t + 1) * E[i - 1][j][t + 1];
+        } else {
+          v = xpb * E[i][j - 1][t];
+          if (t > 0) v += h * E[i][j - 1][t - 1];
+          if (t + 1 <= i + j - 1) v += (t + 1) * E[i][j - 1][t + 1];
+        }
+        E[i][j][t] = v;
+      }
+}
+
+__global__ void k_oneint(int nbf, const int* __restrict__ nprim, const int* __restrict__ off,
+                         const int* __restrict__ lmn, const double* __restrict__ xyz,
+                         const double* __restrict__ exps, const double* __restrict__ nc, int natom,
+                         const double* __restrict__ Z, const double* __restrict__ axyz,
+                         const double* __restrict__ tab, double* __restrict__ S, double* __restrict__ T,
+                         double* __restrict__ V) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nbf * nbf) return;
+  const int pa = idx / nbf, pb = idx % nbf;
+  const int* la = lmn + 3 * pa;
+  const int* lb = lmn + 3 * pb;
+  const double* A = xyz + 3 * pa;
+  const double* B = xyz + 3 * pb;
+  double s = 0.0, t = 0.0, v = 0.0;
+  double Ex[3][5][7], Ey[3][5][7], Ez[3][5][7];
+  double Rc[165], Rn[165], F[9];
+  const double ab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
+  for (int i = 0; i < nprim[pa]; ++i)
+    for (int j = 0; j < nprim[pb]; ++j) {
+      const double a = exps[off[pa] + i], b = exps[off[pb] + j], p = a + b;
+      const double c = nc[off[pa] + i] * nc[off[pb] + j] * exp(-a * b * ab2 / p);
+      const double P[3] = {(a * A[0] + b * B[0]) / p, (a * A[1] + b * B[1]) / p, (a * A[2] + b * B[2]) / p};
+      oe_hermite(p, P[0] - A[0], P[0] - B[0], la[0], lb[0] + 2, Ex);
+      oe_hermite(p, P[1] - A[1], P[1] - B[1], la[1], lb[1] + 2, Ey);
+      oe_hermite(p, P[2] - A[2], P[2] - B[2], la[2], lb[2] + 2, Ez);
+      const double sq = sqrt(M_PI / p);
+      // 1-D overlaps S_d(i, j) = E^{ij}_0 sqrt(pi/p)
+      double sd[3], td[3];
+      double (*E[3])[5][7] = {Ex, Ey, Ez};
+      for (int d = 0; d < 3; ++d) {
+        const int ii = la[d], jj = lb[d];
+        sd[d] = E[d][ii][jj][0] * sq;
+        double k = -2.0 * b * (2 * jj + 1) * E[d][ii][jj][0] + 4.0 * b * b * E[d][ii][jj + 2][0];
+        if (jj >= 2) k += jj * (jj - 1) * E[d][ii][jj - 2][0];
+        td[d] = -0.5 * k * sq;
+      }
+      s += c * sd[0] * sd[1] * sd[2];
+      t += c * (td[0] * sd[1] * sd[2] + sd[0] * td[1] * sd[2] + sd[0] * sd[1] * td[2]);
+      // nuclear attraction
+      const int L = la[0] + lb[0] + la[1] + lb[1] + la[2] + lb[2];
+      for (int at = 0; at < natom; ++at) {
+        const double X = P[0] - axyz[3 * at], Y = P[1] - axyz[3 * at + 1], Zc = P[2] - axyz[3 * at + 2];
+        sqb::boys<8>(p * (X * X + Y * Y + Zc * Zc), tab, F);
+        double base[9], w = 1.0;
+        for (int n = 0; n <= L; ++n) { base[n] = w * F[n]; w *= -2.0 * p; }
+        double* cur = Rc;
+        double* nxt = Rn;
+        cur[0] = base[L];
+        for (int n = L - 1; n >= 0; --n) {
+          for (int N = 0; N <= L - n; ++N)
+            for (int tt = N; tt >= 0; --tt)
+              for (int uu = N - tt; uu >= 0; --uu) {
+                const int vv = N - tt - uu;
+                double r;
+                if (N == 0) r = base[n];
+                else if (tt > 0) r = X * cur[tetra(tt - 1, uu, vv)] + (tt > 1 ? (tt - 1) * cur[tetra(tt - 2, uu, vv)] : 0.0);
+                else if (uu > 0) r = Y * cur[tetra(tt, uu - 1, vv)] + (uu > 1 ? (uu - 1) * cur[tetra(tt, uu - 2, vv)] : 0.0);
+                else r = Zc * cur[tetra(tt, uu, vv - 1)] + (vv > 1 ? (vv - 1) * cur[tetra(tt, uu, vv - 2)] : 0.0);
+                nxt[tetra(tt, uu, vv)] = r;
+              }
+          double* tmp = cur; cur = nxt; nxt = tmp;
+        }
+        double sum = 0.0;
+        for (int tt = 0; tt <= la[0] + lb[0]; ++tt)
+          for (int uu = 0; uu <= la[1] + lb[1]; ++uu)
+            for (int vv = 0; vv <= la[2] + lb[2]; ++vv)
+              sum += Ex[la[0]][lb[0]][tt] * Ey[la[1]][lb[1]][uu] * Ez[la[2]][lb[2]][vv] * cur[tetra(tt, uu, vv)];
+        v -= Z[at] * (2.0 * M_PI / p) * c * sum;
+      }
+    }
+  S[idx] = s;
+  T[idx] = t;
+  V[idx] = v;
+}
+
 int grid_for(long n, int block) {
   long g = (n + block - 1) / block;
   return (int)std::min<long>(std::max<long>(g, 1), 148L * 16);
@@ -1032,5 +1137,62 @@ extern "C" int sqb200_jk_build_noalloc(sqb200_jk* c, const double* dPA, const do
   }
   k_finalize<<<grid_for(nn, 256), 256, 0, st>>>(J, KA, KB, dJT, dKA, dKB, n, uhf);
   CUDA_OK(cudaGetLastError());
+  return SQB200_OK;
+}
+
+
+extern "C" int sqb200_oneint(sqb200_jk* c, int natom, const double* Z, const double* axyz, double* S, double* T,
+                             double* V) {
+  if (!c || natom < 0 || (natom > 0 && (!Z || !axyz)) || !S || !T || !V) return fail(SQB200_EINVAL, "null argument");
+  CUDA_OK(cudaSetDevice(c->device));
+  const int n = c->nbf;
+  std::vector<int> np(n), off(n), lmn(3 * n);
+  std::vector<double> xyz(3 * n), ex, nc;
+  for (const Shell& sh : c->shells)
+    for (int f = 0; f < sh.nfunc; ++f) {
+      const int q = sh.first + f;
+      np[q] = sh.nprim;
+      for (int d = 0; d < 3; ++d) lmn[3 * q + d] = sh.lmn[f][d];
+      xyz[3 * q] = sh.x; xyz[3 * q + 1] = sh.y; xyz[3 * q + 2] = sh.z;
+    }
+  for (int q = 0; q < n; ++q) off[q] = (int)ex.size(), ex.resize(ex.size() + np[q]), nc.resize(nc.size() + np[q]);
+  for (const Shell& sh : c->shells)
+    for (int f = 0; f < sh.nfunc; ++f)
+      for (int k = 0; k < sh.nprim; ++k) {
+        ex[off[sh.first + f] + k] = sh.exps[k];
+        nc[off[sh.first + f] + k] = sh.coef[k][f];
+      }
+  const size_t nn = (size_t)n * n;
+  int *d_np = nullptr, *d_off = nullptr, *d_lmn = nullptr;
+  double *d_xyz = nullptr, *d_ex = nullptr, *d_nc = nullptr, *d_Z = nullptr, *d_A = nullptr, *d_out = nullptr;
+  cudaError_t e = cudaMalloc(&d_np, n * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_off, n * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_lmn, 3 * n * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&d_xyz, 3 * n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_ex, ex.size() * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_nc, nc.size() * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_Z, (natom + 1) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_A, (3 * natom + 3) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_out, 3 * nn * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d_np, np.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_off, off.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_lmn, lmn.data(), 3 * n * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_xyz, xyz.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_ex, ex.data(), ex.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_nc, nc.data(), nc.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && natom > 0) e = cudaMemcpy(d_Z, Z, natom * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && natom > 0) e = cudaMemcpy(d_A, axyz, 3 * natom * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    k_oneint<<<(int)((nn + 127) / 128), 128, 0, c->stream>>>(n, d_np, d_off, d_lmn, d_xyz, d_ex, d_nc, natom, d_Z, d_A,
+                                                              c->d_boys, d_out, d_out + nn, d_out + 2 * nn);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(S, d_out, nn * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(T, d_out + nn, nn * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(V, d_out + 2 * nn, nn * sizeof(double), cudaMemcpyDeviceToHost);
+  void* ptrs[] = {d_np, d_off, d_lmn, d_xyz, d_ex, d_nc, d_Z, d_A, d_out};
+  for (void* q : ptrs) cudaFree(q);
+  if (e != cudaSuccess) return fail(SQB200_ECUDA, std::string("sqb200_oneint: ") + cudaGetErrorString(e));
   return SQB200_OK;
 }

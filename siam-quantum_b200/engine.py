@@ -22,7 +22,8 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 
 EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_jk_build_device",
            "sqb200_jk_stats", "sqb200_jk_profile", "sqb200_jk_profile_read", "sqb200_jk_class_name",
-           "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_jk_set_precision", "sqb200_peak_fma",
+           "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_jk_set_precision", "sqb200_oneint",
+           "sqb200_peak_fma",
            "sqb200_last_error"]
 
 
@@ -53,6 +54,7 @@ def load_library(path=LIB_PATH):
     L.sqb200_jk_profile_read.argtypes = [vp, _f64p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.sqb200_jk_class_name.argtypes = [ctypes.c_int]
     L.sqb200_jk_set_precision.argtypes = [vp, ctypes.c_double]
+    L.sqb200_oneint.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
     L.sqb200_peak_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTS:
@@ -74,6 +76,7 @@ class JKEngine:
     def __init__(self, basis, schwarz=None, device=0):
         L = load_library()
         self.nbf = basis.nbf
+        self.device = device
         self._ctx = ctypes.c_void_p()
         sch = None
         if schwarz is not None:
@@ -119,6 +122,30 @@ class JKEngine:
         _check(_lib.sqb200_jk_build_device(self._ctx, dPA, dPB, int(bool(restricted)), scf_cutoff,
                                            fixed_cutoff, dscreen_rmax, dJT, dKA, dKB, stream))
 
+    def build_tensors(self, PA, PB, JT, KA, KB=None, restricted=True, scf_cutoff=1e-10,
+                      fixed_cutoff=None, dscreen_rmax=float("inf"), stream=None):
+        """build_device on torch tensors (float64, contiguous, (nbf, nbf), on this context's
+        device), enqueued on `stream` (a torch.cuda.Stream; default: torch's current stream).
+        On the legacy default stream (handle 0, which the C ABI reads as the context's own
+        stream) the call synchronises before and after so that torch work stays ordered."""
+        import torch
+        n = self.nbf
+        for t in (PA, PB, JT, KA) + (() if KB is None else (KB,)):
+            if (t.dtype != torch.float64 or not t.is_cuda or t.device.index != self.device
+                    or tuple(t.shape) != (n, n) or not t.is_contiguous()):
+                raise ValueError("build_tensors: need contiguous float64 (%d, %d) tensors on cuda:%d"
+                                 % (n, n, self.device))
+        st = torch.cuda.current_stream(PA.device) if stream is None else stream
+        legacy = st.cuda_stream == 0
+        if legacy:
+            st.synchronize()
+        self.build_device(PA.data_ptr(), PB.data_ptr(), JT.data_ptr(), KA.data_ptr(),
+                          None if KB is None else KB.data_ptr(), restricted=restricted,
+                          scf_cutoff=scf_cutoff, fixed_cutoff=fixed_cutoff,
+                          dscreen_rmax=dscreen_rmax, stream=st.cuda_stream or None)
+        if legacy:
+            self.stats()                           # synchronises the context stream
+
     def stats(self):
         """dict of the last build's counters."""
         out = (ctypes.c_longlong * 6)()
@@ -145,6 +172,16 @@ class JKEngine:
     def set_precision(self, fp32_below):
         """Quartets with Schwarz product below fp32_below use the FP32 kernel form (0 = FP64)."""
         _check(_lib.sqb200_jk_set_precision(self._ctx, float(fp32_below)))
+
+    def oneint(self, charges, coords_bohr):
+        """(S, T, V) one-electron matrices for point charges at coords (bohr)."""
+        n = self.nbf
+        Z = np.ascontiguousarray(charges, dtype=np.float64).reshape(-1)
+        A = np.ascontiguousarray(coords_bohr, dtype=np.float64).reshape(-1)
+        S = np.empty(n * n); T = np.empty(n * n); V = np.empty(n * n)
+        _check(_lib.sqb200_oneint(self._ctx, len(Z), Z if len(Z) else np.zeros(1),
+                                  A if len(A) else np.zeros(3), S, T, V))
+        return S.reshape(n, n), T.reshape(n, n), V.reshape(n, n)
 
     def mem_cutoff(self, fixed_cutoff, max_mem_mb):
         v = ctypes.c_double()

@@ -6,10 +6,12 @@ seeded synthetic molecules and stores, per case, in <case>.npz:
   the reference's own genBasis arrays (nprim, lmn, xyz in bohr, exps, coefs, norms),
   the reference's basis-level Schwarz matrix (create_Schwarz),
   the converged SCF energy and densities PA, PB (uhf(), -SCFACC=1STEP -SCFCONV=1e-8),
+  the reference's one-electron matrices S, T, V (GTO_overlap, GTO_kinetic, GTO_nuclei),
   fresh reference J/K builds from the converged density at cutoff 1e-10:
     *_mem  : -MAXMEM=250 (first visit computes every Schwarz survivor, no density screen)
     *_dir  : -MAXMEM=0   (density screen on every quartet)
 Usage:  make -C oracle && python tests/golden/make_golden.py
+        python tests/golden/make_golden.py --oneint   (add S, T, V to existing fixtures only)
 """
 import os
 import subprocess
@@ -78,6 +80,20 @@ def ref_basis(xyz, bas):
             np.array(coefs), np.array(norms))
 
 
+def add_oneint():
+    for name, geom, bas, opts in CASES:
+        path = os.path.join(OUT, name + ".npz")
+        rec = dict(np.load(path, allow_pickle=True))
+        with tempfile.TemporaryDirectory() as d:
+            xyz = os.path.join(d, "m.xyz")
+            with open(xyz, "w") as f:
+                f.write(M.xyz_text(geom(), name))
+            n = len(rec["nprim"])
+            rec["S"], rec["T"], rec["V"] = port.ref_oneint(xyz, os.path.join(BASIS_DIR, bas + ".txt"), n)
+        np.savez_compressed(path, **rec)
+        print(name, "S/T/V added, nbf", n)
+
+
 def main():
     for name, geom, bas, opts in CASES:
         atoms = geom()
@@ -89,11 +105,12 @@ def main():
             nprim, lmn, xyzs, exps, coefs, norms = ref_basis(xyz, bp)
             n = len(nprim)
             S = port.ref_schwarz(xyz, bp, n)
+            S1, T1, V1 = port.ref_oneint(xyz, bp, n)
             res, PA, PB = port.ref_scf(xyz, bp, ["-SCFACC=1STEP", "-SCFCONV=1e-8"] + list(opts))
             restricted = bool(np.array_equal(PA, PB))
             rec = dict(atoms=np.array(atoms), basis=bas, nprim=nprim, lmn=lmn, xyz=xyzs, exps=exps,
                        coefs=coefs, norms=norms, schwarz=S, energy=res["energy"], PA=PA, PB=PB,
-                       restricted=restricted, cutoff=1e-10)
+                       restricted=restricted, cutoff=1e-10, S=S1, T=T1, V=V1)
             for tag, mm in (("mem", 250), ("dir", 0)):
                 JT, KA, KB, _ = port.ref_jk(xyz, bp, PA, None if restricted else PB,
                                             restricted=restricted, cutoff=1e-10, max_mem=mm)
@@ -103,4 +120,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    add_oneint() if "--oneint" in sys.argv[1:] else main()
