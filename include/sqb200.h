@@ -68,7 +68,7 @@ int sqb200_jk_build_device(sqb200_jk *ctx, const double *dPA, const double *dPB,
  * the implicit device-wide synchronisation of cudaMalloc/cudaFree.  No counterpart in the
  * reference (an addition of this library).  This call allocates nothing: all its scratch
  * (density sum, block maxima, J/K accumulators, counters, work list) lives in one static
- * device array of about 3.5 MB that every GPU loading the library keeps until exit.
+ * device array of about 4 MB that every GPU loading the library keeps until exit.
  * Limits: nbf <= 256 and at most 65536 work items; larger inputs return SQB200_EINVAL with
  * a message.  The context itself (sqb200_jk_create) must already exist.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress) with that device
@@ -110,12 +110,66 @@ const char *sqb200_jk_class_name(int k);
  * counterpart: the reference computes every quartet in FP64. */
 int sqb200_jk_set_precision(sqb200_jk *ctx, double fp32_below);
 
+/* Tile autotuner.  Classes whose ket functions the kernels split into passes have two FP64
+ * forms: the narrow tile (more passes, fewer registers) and the wide tile (fewer passes; each
+ * pass re-derives the Boys function and R for more ket functions).  This call runs the build's
+ * prologue for the given density and cutoffs (as sqb200_jk_build_device) and times both forms
+ * of every such class on the build's own work list (CUDA events, 2 launches each after one
+ * untimed), then keeps the faster form per class for the context's following builds.  Leaves
+ * the context's accumulators dirty (the next build clears them); synchronous.  No reference
+ * counterpart. */
+int sqb200_jk_autotune(sqb200_jk *ctx, const double *dPA, const double *dPB, int restricted,
+                       double scf_cutoff, double fixed_cutoff, double dscreen_rmax, void *stream);
+
+/* Read (sqb200_jk_tiles) or set (sqb200_jk_set_tiles) the per-class tile choice: wide[k] = 1
+ * wide tile, 0 narrow tile, -1 (read only) class k has one form.  sqb200_jk_tiles returns the
+ * number of entries written (at most n). */
+int sqb200_jk_tiles(sqb200_jk *ctx, int *wide, int n);
+int sqb200_jk_set_tiles(sqb200_jk *ctx, const int *wide, int n);
+
 /* One-electron integrals of the context's basis on its device: overlap S, kinetic T and
  * nuclear attraction V = -sum_C Z_C <p|1/|r-C||q> for natom point charges Z at axyz (bohr),
  * each written to a host nbf*nbf array (the matrices the reference's uhf() builds with
  * overlap/kinetic/nai, src/uhf.c:1307-1334; H = T + V). */
 int sqb200_oneint(sqb200_jk *ctx, int natom, const double *Z, const double *axyz,
                   double *S, double *T, double *V);
+
+/* ---- Batched builds: many molecules' J/K in one launch per class kernel. ----
+ * No reference counterpart (the reference builds one molecule per process); each molecule's
+ * result is the single-molecule build of its own context (same screening, same sums up to
+ * the order of floating-point additions). */
+typedef struct sqb200_batch sqb200_batch;
+
+/* Join nmol contexts (sqb200_jk_create, all on one device) into a batch.  The batch copies
+ * their pair data into merged per-class arrays; the contexts must outlive the batch (their
+ * Boys table, shells and FP32 threshold are read).  Packed layout of every batched matrix:
+ * molecule m's nbf_m x nbf_m row-major block starts at element off[m] (sqb200_batch_offsets). */
+int sqb200_batch_create(sqb200_batch **batch, int nmol, sqb200_jk *const *ctxs);
+int sqb200_batch_destroy(sqb200_batch *batch);
+
+/* off[0..nmol]: off[m] = sum of nbf_k^2 for k < m; off[nmol] = total elements. */
+int sqb200_batch_offsets(sqb200_batch *batch, long long *off);
+
+/* Per-molecule spin and cutoffs of the next builds (arrays of nmol), with the meaning of
+ * sqb200_jk_build's restricted / scf_cutoff / fixed_cutoff / dscreen_rmax.  Synchronises the
+ * batch's streams and rebuilds the work list when a spin or Schwarz cutoff changed. */
+int sqb200_batch_set_step(sqb200_batch *batch, const int *restricted, const double *scf_cutoff,
+                          const double *fixed_cutoff, const double *dscreen_rmax);
+
+/* One build of every molecule on packed device arrays, enqueued on `stream` (NULL = the batch's
+ * own stream), not synchronised, no host work and no allocation: capturable into a CUDA graph.
+ * For a restricted molecule its PB block must equal its PA block (the reference passes PA as
+ * both spins) and its KB block receives KA. */
+int sqb200_batch_build_device(sqb200_batch *batch, const double *dPA, const double *dPB,
+                              double *dJT, double *dKA, double *dKB, void *stream);
+
+/* The tile autotuner of sqb200_jk_autotune on a batch's work list of the current step (each
+ * class keeps the form whose summed time over both spins is lower). */
+int sqb200_batch_autotune(sqb200_batch *batch, const double *dPA, const double *dPB, void *stream);
+
+/* Counters of the last batched build, as sqb200_jk_stats (summed over molecules).
+ * Synchronises with the device. */
+int sqb200_batch_stats(sqb200_batch *batch, long long *out, int n);
 
 /* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,
  * src/matrix.c:389-440), written to the host array S (nbf*nbf). */

@@ -6,9 +6,10 @@ Python package is the host-side binding used by tests and the benchmark:
   basis      genBasis-order Cartesian Gaussian basis builder (flat arrays for the ABI)
   molecules  seeded workload geometries (water, benzene, C60, random organics)
   scf        device-resident RHF/UHF SCF around the GPU Fock build (SCFJob)
+  batch_scf  many molecules' SCF together: batched Fock builds in a CUDA graph (BatchSCF)
 
 The directory name is not a Python identifier; import it with `load_package()` from a
 checkout root or via importlib (see tests/conftest.py).
 """
-from . import basis, engine, molecules, scf  # noqa: F401
-from .engine import JKEngine, SQB200Error, load_library  # noqa: F401
+from . import basis, batch_scf, engine, molecules, scf  # noqa: F401
+from .engine import JKBatch, JKEngine, SQB200Error, load_library  # noqa: F401

@@ -49,8 +49,13 @@ PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
 # bra/ket orientation: the larger pair (by functions, then L) is the bra
 PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
 STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out accumulators per pass
+# the wide tile: a second FP64 form of every class whose passes it merges (fewer passes, each
+# re-deriving the Boys function and R for more ket functions, at more registers); which form a
+# class runs is chosen by measurement (sqb200_jk_autotune)
+STATE_MAX_WIDE = int(os.environ.get("SQB_STATE_MAX_WIDE", "128"))
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
 F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
+MIN_BLOCKS = int(os.environ.get("SQB_MINB", "0"))   # __launch_bounds__ min CTAs per SM (0 = none)
 USE_WS = int(os.environ.get("SQB_WS", "0"))   # also emit warp-specialised multi-pass kernels (measured slower on B200; opt-in)
 CTA = 128
 
@@ -142,7 +147,31 @@ def boys_flops(M):
     return 8 * 3 + M * 3
 
 
-def gen_class(bra, ket, spin, prec="D"):
+def alg_prim_flops(fk, Hb, rt, fma):
+    """Algorithmic operations per primitive quartet of a class: the pass-free algorithm (primitive
+    setup, one Boys evaluation at the class's highest Hermite order, every R value once, every
+    ket E contraction once).  Passes that re-derive the Boys function and R for another block
+    of ket functions emit more operations than this; those repeats are not counted as work."""
+    need, ncons = set(), 0
+    for f in fk:
+        for (tau, nu, phi) in nz(f):
+            for h in Hb:
+                need.add((h[0] + tau, h[1] + nu, h[2] + phi))
+                ncons += 1
+    L = max(sum(x) for x in need)
+    _, rf = gen_R(Emitter(), L, need, rt=rt, fma=fma)
+    return 9 + 2 + 3 + 5 + boys_flops(L) + 2 + L + (L + 1) + rf + 2 * ncons
+
+
+def n_passes(bra, ket, state_max):
+    fb, _, _ = etable(bra)
+    fk, _, _ = etable(ket)
+    Hb = {h for f in fb for h in nz(f)}
+    per = max(1, state_max // (len(Hb) + len(fb)))
+    return (len(fk) + per - 1) // per
+
+
+def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
     """Return (kernel source, metadata) for class (bra|ket) and spin 'R' or 'U'.  prec "F"
     emits the mixed form: primitive setup, prefactor cut and Boys function in FP64, Hermite
     integrals, E tables and contracted accumulators in FP32, digestion into the FP64 J/K
@@ -161,14 +190,16 @@ def gen_class(bra, ket, spin, prec="D"):
     nc, nd = len(COMP[ket[0]]), len(COMP[ket[1]])
     NB = 5 + len(layb)
     NK = 5 + len(layk)
-    per = max(1, STATE_MAX // (len(Hb) + nab))
+    per = max(1, (STATE_MAX if state_max is None else state_max) // (len(Hb) + nab))
     blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
-    name = "jk_%s_%s_%s%s" % (bra, ket, spin, "_f32" if F32 else "")
-    fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks)}
+    name = "jk_%s_%s_%s%s%s" % (bra, ket, spin, "_f32" if F32 else "", suffix)
+    fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks),
+          "alg_prim": alg_prim_flops(fk, Hb, RT, FMA)}
 
     em = Emitter()
     out = []
-    out.append('extern "C" __global__ void __launch_bounds__(%d)' % CTA)
+    out.append('extern "C" __global__ void __launch_bounds__(%s)' % (
+        "%d, %d" % (CTA, MIN_BLOCKS) if MIN_BLOCKS else "%d" % CTA))
     out.append("%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name)
     if F32:
         em("extern __shared__ float sbra_f32[];")
@@ -177,7 +208,11 @@ def gen_class(bra, ket, spin, prec="D"):
         em("extern __shared__ double sbra[];")
     em("const sqb::WorkItem it = items[blockIdx.x];")
     em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
-    em("const int N = a.nbf;")
+    em("const sqb::MolRec mr = a.mols[it.mol];        // the molecule of this work item")
+    em("double* __restrict__ Jacc = a.Jacc + mr.moff;")
+    em("double* __restrict__ KAacc = a.KAacc + mr.moff;")
+    em("double* __restrict__ KBacc = a.KBacc + mr.moff;")
+    em("const int N = mr.nbf;")
     em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims%s[bp.poff + x];" % (NB, "_f" if F32 else ""))
     em("__syncthreads();")
     em("const int isplit = it.isplit;                 // threads sharing one quartet (bra primitives split)")
@@ -190,13 +225,13 @@ def gen_class(bra, ket, spin, prec="D"):
     em.ind += 1
     em("kp = a.ket_pairs[it.k0 + kl];")
     em("const double r = bp.schwarz * kp.schwarz;")
-    em("ok = !(r < a.cut_outer) && !(r < a.cut_fixed);")
-    em("if (ok && r < a.dscreen_rmax) {")
+    em("ok = !(r < mr.cut_outer) && !(r < mr.cut_fixed);")
+    em("if (ok && r < mr.dscreen_rmax) {")
     em("  const bool bf = (bp.P > kp.P) || (bp.P == kp.P && bp.Q >= kp.Q);")
     em("  const int P = bf ? bp.P : kp.P, Q = bf ? bp.Q : kp.Q, I = bf ? kp.P : bp.P, J = bf ? kp.Q : bp.Q;")
-    em("  const double* PM = a.PM; const int ns = a.ns;")
+    em("  const double* PM = a.PM + mr.pmoff; const int ns = mr.ns;")
     em("  const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];")
-    em("  ok = !(r * mp < a.cut_fixed);")
+    em("  ok = !(r * mp < mr.cut_fixed);")
     em("}")
     em("deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + kl) ? 0.5 : 1.0);")
     em.ind -= 1
@@ -209,10 +244,10 @@ def gen_class(bra, ket, spin, prec="D"):
     em("const %s* __restrict__ kprim = a.ket_prims%s + kp.poff;" % (RT, "_f" if F32 else ""))
     em("const int nbp = bp.nprim, nkp = kp.nprim;")
     em("nflush = pass == 0 ? (unsigned long long)((nbp - grp + isplit - 1) / isplit) : 0ull;")
-    em("const double* __restrict__ PA = a.PA;")
+    em("const double* __restrict__ PA = a.PA + mr.moff;")
     if spin == "U":
-        em("const double* __restrict__ PB = a.PB;")
-    em("const double* __restrict__ PT = a.PT;")
+        em("const double* __restrict__ PB = a.PB + mr.moff;")
+    em("const double* __restrict__ PT = a.PT + mr.moff;")
     em("switch (pass) {")
     for bi, blk in enumerate(blocks):
         em("case %d: {  // ket functions %s" % (bi, blk))
@@ -332,7 +367,7 @@ def gen_class(bra, ket, spin, prec="D"):
     em("  const double s2 = 2.0 * deg;")
     for ab in range(nab):
         aa, bb = divmod(ab, nb_)
-        em("  { const double v = sqb::warp_sum(s2 * jab%d); if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(a.Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
+        em("  { const double v = sqb::warp_sum(s2 * jab%d); if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
     em("}")
     em("sqb::count_add(a.counters + 0, (ok && grp == 0 && pass == 0) ? 1ull : 0ull);")
     em("sqb::count_add(a.counters + 1, nprimq);")
@@ -381,10 +416,10 @@ def emit_digest(em, spin, blk, nab, na, nb_, nd):
     for cd in blk:
         c, d = divmod(cd, nd)
         terms = " + ".join("o%d_%d * ptb%d" % (ab, cd, ab) for ab in range(nab))
-        em("atomicAdd(a.Jacc + (fI + %d) * N + fJ + %d, 2.0 * deg * (%s));" % (c, d, terms))
+        em("atomicAdd(Jacc + (fI + %d) * N + fJ + %d, 2.0 * deg * (%s));" % (c, d, terms))
         qf += 2 * nab + 2
     for s, _ in spins:
-        acc = "a.KAacc" if s == "A" else "a.KBacc"
+        acc = "KAacc" if s == "A" else "KBacc"
         tg = {}
         for ab in range(nab):
             aa, bb = divmod(ab, nb_)
@@ -452,7 +487,11 @@ def gen_class_ws(bra, ket, spin):
     em("double* __restrict__ sbra = smem + %d;" % (P * NR * 32))
     em("const sqb::WorkItem it = items[blockIdx.x];")
     em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
-    em("const int N = a.nbf;")
+    em("const sqb::MolRec mr = a.mols[it.mol];        // the molecule of this work item")
+    em("double* __restrict__ Jacc = a.Jacc + mr.moff;")
+    em("double* __restrict__ KAacc = a.KAacc + mr.moff;")
+    em("double* __restrict__ KBacc = a.KBacc + mr.moff;")
+    em("const int N = mr.nbf;")
     em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
     em("__syncthreads();")
     em("const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;")
@@ -461,22 +500,22 @@ def gen_class_ws(bra, ket, spin):
     em("double deg = 0.0;")
     em("if (ok) {")
     em("  const double r = bp.schwarz * kp.schwarz;")
-    em("  ok = !(r < a.cut_outer) && !(r < a.cut_fixed);")
-    em("  if (ok && r < a.dscreen_rmax) {")
+    em("  ok = !(r < mr.cut_outer) && !(r < mr.cut_fixed);")
+    em("  if (ok && r < mr.dscreen_rmax) {")
     em("    const bool bf = (bp.P > kp.P) || (bp.P == kp.P && bp.Q >= kp.Q);")
     em("    const int P = bf ? bp.P : kp.P, Q = bf ? bp.Q : kp.Q, I = bf ? kp.P : bp.P, J = bf ? kp.Q : bp.Q;")
-    em("    const double* PM = a.PM; const int ns = a.ns;")
+    em("    const double* PM = a.PM + mr.pmoff; const int ns = mr.ns;")
     em("    const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];")
-    em("    ok = !(r * mp < a.cut_fixed);")
+    em("    ok = !(r * mp < mr.cut_fixed);")
     em("  }")
     em("  deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + lane) ? 0.5 : 1.0);")
     em("}")
     em("const int nbp = bp.nprim, nkp = kp.nprim, S = nbp * nkp;   // uniform over the CTA")
     em("const double* __restrict__ kprim = a.ket_prims + kp.poff;")
-    em("const double* __restrict__ PA = a.PA;")
+    em("const double* __restrict__ PA = a.PA + mr.moff;")
     if spin == "U":
-        em("const double* __restrict__ PB = a.PB;")
-    em("const double* __restrict__ PT = a.PT;")
+        em("const double* __restrict__ PB = a.PB + mr.moff;")
+    em("const double* __restrict__ PT = a.PT + mr.moff;")
     for ab in range(nab):
         em("double jab%d = 0.0;" % ab)
     em("unsigned long long nprimq = 0;")
@@ -611,7 +650,7 @@ def gen_class_ws(bra, ket, spin):
     em("  const double s2 = 2.0 * deg;")
     for ab in range(nab):
         aa, bb = divmod(ab, nb_)
-        em("  { const double v = sqb::warp_sum(s2 * jab%d); if (lane == 0 && v != 0.0) atomicAdd(a.Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
+        em("  { const double v = sqb::warp_sum(s2 * jab%d); if (lane == 0 && v != 0.0) atomicAdd(Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
     em("}")
     em("sqb::count_add(a.counters + 0, (ok && wp == 0) ? 1ull : 0ull);")
     em("sqb::count_add(a.counters + 1, nprimq);")
@@ -652,6 +691,11 @@ def main():
                 s2, m2 = gen_class_ws(bra, ket, spin)
                 src.append(s2)
                 m["ws"] = m2
+            m["wide"] = None
+            if n_passes(bra, ket, STATE_MAX_WIDE) < n_passes(bra, ket, STATE_MAX):
+                s4, m4 = gen_class(bra, ket, spin, "D", STATE_MAX_WIDE, "_w")
+                src.append(s4)
+                m["wide"] = m4
             m["f32"] = None
             if pair_L(bra) + pair_L(ket) <= F32_MAX_L:
                 s3, m3 = gen_class(bra, ket, spin, "F")
@@ -670,6 +714,8 @@ def main():
             reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["ws"]["name"])
         if m["f32"]:
             reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["f32"]["name"])
+        if m["wide"]:
+            reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["wide"]["name"])
     reg.append("")
     reg.append("namespace sqb {")
     reg.append("const char* const kPairClassNames[%d] = {%s};" % (len(PAIRS), ", ".join('"%s"' % p for p in PAIRS)))
@@ -689,9 +735,17 @@ def main():
             reg.append('   0, 0, nullptr, nullptr, 0, 0, 0,')
         fr, fu = r["f32"], u["f32"]
         if fr:
-            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d,' % (
                 fr["flops"]["passes"], fr["name"], fu["name"], fr["flops"]["prim"], fr["flops"]["flush"],
                 fr["flops"]["quartet"]))
+        else:
+            reg.append('   0, nullptr, nullptr, 0, 0, 0,')
+        reg.append('   %d,' % r["flops"]["alg_prim"])
+        wr, wu = r["wide"], u["wide"]
+        if wr:
+            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+                wr["flops"]["passes"], wr["name"], wu["name"], wr["flops"]["prim"], wr["flops"]["flush"],
+                wr["flops"]["quartet"]))
         else:
             reg.append('   0, nullptr, nullptr, 0, 0, 0},')
     reg.append("};")
@@ -702,6 +756,7 @@ def main():
     fj = {m["name"]: m["flops"] for m in metas}
     fj.update({m["ws"]["name"]: m["ws"]["flops"] for m in metas if m["ws"]})
     fj.update({m["f32"]["name"]: m["f32"]["flops"] for m in metas if m["f32"]})
+    fj.update({m["wide"]["name"]: m["wide"]["flops"] for m in metas if m["wide"]})
     write_if_changed(os.path.join(outdir, "jk_flops.json"), json.dumps(fj, indent=0))
     write_if_changed(os.path.join(outdir, "files.txt"), "\n".join(files) + "\n")
     print("generated %d kernels in %d files" % (len(metas), len(files)))

@@ -37,6 +37,19 @@ struct PairRec {
 // handled by `isplit` threads (power of two) that split the bra primitives between them.
 struct WorkItem {
   int bra, k0, cnt, isplit;
+  int mol;         // index of the molecule (MolRec) the pairs belong to
+};
+
+// One molecule of a build: where its matrices sit in the packed device arrays, and the
+// cutoffs of its current SCF step.  A single-molecule build has one record at offset 0; a
+// batched build packs many molecules' nbf x nbf blocks back to back.
+struct MolRec {
+  long long moff;      // offset (doubles) of its nbf x nbf blocks in PA, PB, PT, Jacc, KAacc, KBacc
+  long long pmoff;     // offset of its ns x ns block-maximum matrix in PM
+  int nbf, ns;
+  double cut_outer, cut_fixed, dscreen_rmax;
+  int shoff;           // its first shell in the packed shell tables (batched block maxima)
+  int uhf;             // 1 = unrestricted (KB from PB), 0 = restricted (KB = KA)
 };
 
 struct JKArgs {
@@ -47,17 +60,16 @@ struct JKArgs {
   const double* PA;
   const double* PB;
   const double* PT;
-  const double* PM;            // ns x ns shell-block max of |PT|,|PA|,|PB|
-  double* Jacc;                // nbf x nbf, J = Jacc + Jacc^T
-  double* KAacc;               // nbf x nbf, K[PA] = KAacc + KAacc^T
+  const double* PM;            // per molecule ns x ns shell-block max of |PT|,|PA|,|PB|
+  double* Jacc;                // per molecule nbf x nbf, J = Jacc + Jacc^T
+  double* KAacc;               // per molecule nbf x nbf, K[PA] = KAacc + KAacc^T
   double* KBacc;
   const double* boys_tab;      // BOYS_NGRID x BOYS_NCOL
   unsigned long long* counters;// [0] quartets computed, [1] primitive quartets evaluated,
                                // [2] bra-primitive flushes, [3] digestions
-  int nbf, ns;
+  const MolRec* mols;          // per-molecule offsets, sizes and cutoffs (WorkItem::mol)
   int same_class;              // bra and ket pairs come from one class (pair identity possible)
   int pad;
-  double cut_outer, cut_fixed, dscreen_rmax;
   const float* bra_prims_f;    // FP32 copies of the primitive records (mixed-precision kernels)
   const float* ket_prims_f;
 };

@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -201,13 +202,15 @@ struct sqb200_jk {
   double *d_PA = nullptr, *d_PB = nullptr, *d_PT = nullptr, *d_PM = nullptr;
   double *d_J = nullptr, *d_KA = nullptr, *d_KB = nullptr;
   double *d_JT = nullptr, *d_KAo = nullptr, *d_KBo = nullptr;   // outputs for host builds
-  unsigned long long* d_counters = nullptr;  // 3 per class kernel
+  unsigned long long* d_counters = nullptr;  // 4 per class kernel form
+  sqb::MolRec* d_mol = nullptr;              // the build's molecule record (written by k_prep)
   // work lists cached per (outer, fixed) cutoff
   // a segment's kernel index v < K is the FP64 form of class v, v >= K the FP32 form of
   // class v - K (K = kNumClassKernels); counters and timings use the same index
   struct Work {
     std::vector<int> kernel;      // kernel index per segment
     std::vector<int> first, count;
+    std::vector<double> cost;     // estimated FP operations per segment (launch order, stream choice)
     sqb::WorkItem* d_items = nullptr;
     int total = 0;
   };
@@ -215,9 +218,16 @@ struct sqb200_jk {
   double fp32_below = 0.0;      // quartets with Schwarz product below this use the FP32 form
   bool use_ws = true;           // warp-specialised form where a class has one (SQB200_WS=0 disables)
   std::vector<char> ran_ws;     // per class kernel: which form the last build launched
+  std::vector<char> wide;       // per class kernel: run the wide-tile FP64 form (sqb200_jk_autotune)
   std::vector<long long> last_counts;
   long long last_flops = 0;
   int last_launches = 0;        // kernels enqueued by the last build
+  // side streams for concurrent class launches: the build forks them off its stream after the
+  // prologue and joins them before k_finalize (SQB200_STREAMS, default 4; 0 = one stream)
+  int nside = -1;
+  std::vector<cudaStream_t> side;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
   // per-class event timing (sqb200_jk_profile)
   bool profile = false;
   struct Ev { int kernel; cudaEvent_t a, b; };
@@ -230,8 +240,12 @@ namespace {
 
 // ---------------------------------------------------------------- device helpers
 
+// PT = PA + PB and zeroed accumulators; the first thread also writes the build's molecule
+// record (offsets 0, sizes and this build's cutoffs), which the class kernels read
 __global__ void k_prep(const double* __restrict__ PA, const double* __restrict__ PB, double* __restrict__ PT,
-                       double* __restrict__ J, double* __restrict__ KA, double* __restrict__ KB, int nn, int uhf) {
+                       double* __restrict__ J, double* __restrict__ KA, double* __restrict__ KB, int nn, int uhf,
+                       sqb::MolRec* __restrict__ mol, sqb::MolRec mv) {
+  if (mol && blockIdx.x == 0 && threadIdx.x == 0) *mol = mv;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
     PT[i] = PA[i] + PB[i];
     J[i] = 0.0;
@@ -601,6 +615,85 @@ int upload_pairs(sqb200_jk* c) {
 }
 
 // Work list: per class kernel, one item per (bra pair, <=128 ket pairs).
+int ensure_side_streams(sqb200_jk* c) {
+  if (c->nside >= 0) return SQB200_OK;
+  int n = 4;
+  if (const char* e = getenv("SQB200_STREAMS")) n = std::max(0, std::min(16, atoi(e)));
+  CUDA_OK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  for (int i = 0; i < n; ++i) {
+    cudaStream_t s;
+    cudaEvent_t e;
+    CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    c->side.push_back(s);
+    c->ev_join.push_back(e);
+  }
+  c->nside = n;
+  return SQB200_OK;
+}
+
+// Work items of class kernel ki for one molecule (context c): every surviving (bra pair, <=kper
+// ket pairs) unit, with pair indices shifted by bra_base/ket_base (the molecule's first pair in
+// a merged class array; 0 for a single-molecule build).  Kets whose Schwarz product is below the
+// context's fp32_below go to items32 (the FP32 form).  cost64/cost32 accumulate the emitted
+// operations, the launch-order and stream-balancing estimate.
+void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra_base, int ket_base, int mol,
+                 std::vector<sqb::WorkItem>& items, std::vector<sqb::WorkItem>& items32, double& cost64,
+                 double& cost32) {
+  const sqb::ClassKernel& K = sqb::kClassKernels[ki];
+  const PairClass& B = c->cls[K.bra_cls];
+  const PairClass& T = c->cls[K.ket_cls];
+  if (B.pairs.empty() || T.pairs.empty()) return;
+  const double cut = std::max(outer, fixed);
+  const bool same = K.bra_cls == K.ket_cls;
+  const bool mixed = c->fp32_below > 0.0 && K.fn_r32 != nullptr;
+  // every (bra sub-list, ket sub-list) combination; inside one class each unordered pair of
+  // sub-lists once, and inside one sub-list each unordered pair of pairs once (k >= b)
+  for (size_t sx = 0; sx + 1 < B.sub.size(); ++sx)
+    for (size_t sy = 0; sy + 1 < T.sub.size(); ++sy) {
+      if (same && sx > sy) continue;
+      const int b0 = B.sub[sx], b1 = B.sub[sx + 1], k0s = T.sub[sy], k1s = T.sub[sy + 1];
+      const int nbp = B.pairs[b0].nprim, nkp = T.pairs[k0s].nprim;
+      // split the bra primitives over up to 32 threads when a quartet has many primitives
+      // (the warp-specialised form takes 32 kets per CTA, one lane each)
+      const bool ws = c->use_ws && K.ws_r != nullptr;
+      int isplit = 1;
+      while (!ws && isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
+      const int kper = ws ? 32 : 128 / isplit;
+      const double pq = (double)nbp * nkp;
+      for (int b = b0; b < b1; ++b) {
+        const double sb = B.pairs[b].schwarz;
+        if (!(sb > 0.0)) break;   // sorted: the rest are zero
+        const double thr = cut / sb * (1.0 - 1e-12);
+        // ket pairs of the sub-list with schwarz >= thr form a prefix of it
+        int lo = k0s, hi = k1s;
+        while (lo < hi) {
+          const int mid = (lo + hi) / 2;
+          if (T.pairs[mid].schwarz >= thr) lo = mid + 1; else hi = mid;
+        }
+        const int end = lo;
+        const int start = (same && sx == sy) ? b : k0s;
+        // kets with Sch(bra)*Sch(ket) >= fp32_below (a prefix) stay FP64, the rest go FP32
+        int mid = end;
+        if (mixed) {
+          const double t32 = c->fp32_below / sb;
+          int l2 = start, h2 = end;
+          while (l2 < h2) {
+            const int m2 = (l2 + h2) / 2;
+            if (T.pairs[m2].schwarz >= t32) l2 = m2 + 1; else h2 = m2;
+          }
+          mid = l2;
+        }
+        for (int k0 = start; k0 < mid; k0 += kper)
+          items.push_back({bra_base + b, ket_base + k0, std::min(kper, mid - k0), isplit, mol});
+        for (int k0 = std::max(start, mid); k0 < end; k0 += kper)
+          items32.push_back({bra_base + b, ket_base + k0, std::min(kper, end - k0), isplit, mol});
+        cost64 += std::max(0, mid - start) * (pq * K.flops_prim + K.flops_quartet);
+        cost32 += std::max(0, end - std::max(start, mid)) * (pq * K.f32_flops_prim + K.f32_flops_quartet);
+      }
+    }
+}
+
 int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) {
   auto key = std::make_tuple(outer, fixed, c->fp32_below);
   auto it = c->work.find(key);
@@ -610,67 +703,23 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
   }
   sqb200_jk::Work w;
   std::vector<sqb::WorkItem> items, items32;
-  const double cut = std::max(outer, fixed);
   for (int ki = 0; ki < sqb::kNumClassKernels; ++ki) {
-    const sqb::ClassKernel& K = sqb::kClassKernels[ki];
-    const PairClass& B = c->cls[K.bra_cls];
-    const PairClass& T = c->cls[K.ket_cls];
-    if (B.pairs.empty() || T.pairs.empty()) continue;
     const int first = (int)items.size();
-    const bool same = K.bra_cls == K.ket_cls;
-    const bool mixed = c->fp32_below > 0.0 && K.fn_r32 != nullptr;
     items32.clear();
-    // every (bra sub-list, ket sub-list) combination; inside one class each unordered pair of
-    // sub-lists once, and inside one sub-list each unordered pair of pairs once (k >= b)
-    for (size_t sx = 0; sx + 1 < B.sub.size(); ++sx)
-      for (size_t sy = 0; sy + 1 < T.sub.size(); ++sy) {
-        if (same && sx > sy) continue;
-        const int b0 = B.sub[sx], b1 = B.sub[sx + 1], k0s = T.sub[sy], k1s = T.sub[sy + 1];
-        const int nbp = B.pairs[b0].nprim, nkp = T.pairs[k0s].nprim;
-        // split the bra primitives over up to 32 threads when a quartet has many primitives
-        // (the warp-specialised form takes 32 kets per CTA, one lane each)
-        const bool ws = c->use_ws && K.ws_r != nullptr;
-        int isplit = 1;
-        while (!ws && isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
-        const int kper = ws ? 32 : 128 / isplit;
-        for (int b = b0; b < b1; ++b) {
-          const double sb = B.pairs[b].schwarz;
-          if (!(sb > 0.0)) break;   // sorted: the rest are zero
-          const double thr = cut / sb * (1.0 - 1e-12);
-          // ket pairs of the sub-list with schwarz >= thr form a prefix of it
-          int lo = k0s, hi = k1s;
-          while (lo < hi) {
-            const int mid = (lo + hi) / 2;
-            if (T.pairs[mid].schwarz >= thr) lo = mid + 1; else hi = mid;
-          }
-          const int end = lo;
-          const int start = (same && sx == sy) ? b : k0s;
-          // kets with Sch(bra)*Sch(ket) >= fp32_below (a prefix) stay FP64, the rest go FP32
-          int mid = end;
-          if (mixed) {
-            const double t32 = c->fp32_below / sb;
-            int l2 = start, h2 = end;
-            while (l2 < h2) {
-              const int m2 = (l2 + h2) / 2;
-              if (T.pairs[m2].schwarz >= t32) l2 = m2 + 1; else h2 = m2;
-            }
-            mid = l2;
-          }
-          for (int k0 = start; k0 < mid; k0 += kper) items.push_back({b, k0, std::min(kper, mid - k0), isplit});
-          for (int k0 = std::max(start, mid); k0 < end; k0 += kper)
-            items32.push_back({b, k0, std::min(kper, end - k0), isplit});
-        }
-      }
+    double cost64 = 0.0, cost32 = 0.0;
+    class_items(c, ki, outer, fixed, 0, 0, 0, items, items32, cost64, cost32);
     const int cnt = (int)items.size() - first;
     if (cnt > 0) {
       w.kernel.push_back(ki);
       w.first.push_back(first);
       w.count.push_back(cnt);
+      w.cost.push_back(cost64);
     }
     if (!items32.empty()) {
       w.kernel.push_back(ki + sqb::kNumClassKernels);
       w.first.push_back((int)items.size());
       w.count.push_back((int)items32.size());
+      w.cost.push_back(cost32);
       items.insert(items.end(), items32.begin(), items32.end());
     }
   }
@@ -684,6 +733,87 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
   return SQB200_OK;
 }
 
+// One class-kernel launch of a work segment, ready to enqueue.
+struct SegLaunch {
+  const void* fn = nullptr;
+  dim3 grid, block;
+  size_t smem = 0;
+  sqb::JKArgs a;
+  const sqb::WorkItem* items = nullptr;
+};
+
+// The form of class kernel v (v >= K: FP32 form) for spin uhf; wide selects the wide-tile FP64
+// form where the class has one.
+void pick_form(const sqb::ClassKernel& K, bool f32, int uhf, bool wide, const void** fn, int* passes) {
+  if (f32) { *fn = uhf ? K.fn_u32 : K.fn_r32; *passes = K.passes32; return; }
+  if (wide && K.fn_rw) { *fn = uhf ? K.fn_uw : K.fn_rw; *passes = K.passes_w; return; }
+  *fn = uhf ? K.fn_u : K.fn_r;
+  *passes = K.passes;
+}
+
+// Raise a kernel's dynamic shared-memory limit once per (device, kernel, size class), so that a
+// build captured into a CUDA graph after a first uncaptured build issues only stream work.
+int ensure_smem(const void* fn, size_t smem) {
+  if (smem <= 48 * 1024) return SQB200_OK;
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> done;
+  int dev = 0;
+  CUDA_OK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = done[{dev, fn}];
+  if (have >= smem) return SQB200_OK;
+  CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  have = smem;
+  return SQB200_OK;
+}
+
+int enqueue(const SegLaunch& L, cudaStream_t st) {
+  sqb::JKArgs a = L.a;
+  const sqb::WorkItem* items = L.items;
+  void* args[] = {&a, &items};
+  const int rc = ensure_smem(L.fn, L.smem);
+  if (rc) return rc;
+  CUDA_OK(cudaLaunchKernel(L.fn, L.grid, L.block, args, L.smem, st));
+  return SQB200_OK;
+}
+
+// Segment s of a single-context work list; wide < 0 takes the context's tile choice.
+SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const double* dPA, const double* dPB,
+                     int uhf, int wide) {
+  SegLaunch L;
+  const int v = w->kernel[s];
+  const bool f32 = v >= sqb::kNumClassKernels;
+  const int kidx = f32 ? v - sqb::kNumClassKernels : v;
+  const sqb::ClassKernel& K = sqb::kClassKernels[kidx];
+  const PairClass& B = c->cls[K.bra_cls];
+  const PairClass& T = c->cls[K.ket_cls];
+  sqb::JKArgs& a = L.a;
+  memset(&a, 0, sizeof(a));
+  a.bra_pairs = B.d_pairs; a.bra_prims = B.d_prims;
+  a.ket_pairs = T.d_pairs; a.ket_prims = T.d_prims;
+  a.PA = dPA; a.PB = dPB; a.PT = c->d_PT; a.PM = c->d_PM;
+  a.Jacc = c->d_J; a.KAacc = c->d_KA; a.KBacc = c->d_KB;
+  a.boys_tab = c->d_boys;
+  a.counters = c->d_counters + 4 * v;
+  a.bra_prims_f = B.d_primsf; a.ket_prims_f = T.d_primsf;
+  a.mols = c->d_mol;
+  a.same_class = K.bra_cls == K.ket_cls;
+  L.items = w->d_items + w->first[s];
+  const bool ws = !f32 && c->use_ws && K.ws_r != nullptr;
+  if (!f32) c->ran_ws[kidx] = ws;
+  L.smem = (size_t)B.max_nprim * B.stride * (f32 ? sizeof(float) : sizeof(double)) +
+           (ws ? (size_t)K.ws_warps * K.ws_nr * 32 * sizeof(double) : 0);
+  int passes = 1;
+  if (ws) {
+    L.fn = uhf ? K.ws_u : K.ws_r;
+  } else {
+    pick_form(K, f32, uhf, wide < 0 ? (c->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
+  }
+  L.grid = dim3(w->count[s], passes);
+  L.block = dim3(ws ? 32 * K.ws_warps : 128);
+  return L;
+}
+
 int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restricted, double outer,
                  double fixed, double dscreen, double* dJT, double* dKA, double* dKB, cudaStream_t st) {
   const int n = c->nbf, nn = n * n;
@@ -693,49 +823,49 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   sqb200_jk::Work* w = nullptr;
   int rc = build_work(c, outer, fixed, &w);
   if (rc) return rc;
-  k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf);
+  const sqb::MolRec mv{0, 0, n, c->ns, outer, fixed, dscreen, 0, uhf};
+  k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf, c->d_mol, mv);
   k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM);
   CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 8 * sqb::kNumClassKernels, st));
   c->last_launches = 3 + (int)w->kernel.size();
-  for (size_t s = 0; s < w->kernel.size(); ++s) {
+  // segments largest first, each on the least-loaded lane (lane 0 = st, the others are side
+  // streams forked off st); per-class profiling keeps every launch on st so that each event
+  // pair times one kernel alone
+  rc = ensure_side_streams(c);
+  if (rc) return rc;
+  const int nlanes = c->profile ? 1 : 1 + c->nside;
+  std::vector<size_t> order(w->kernel.size());
+  for (size_t s = 0; s < order.size(); ++s) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return w->cost[x] > w->cost[y]; });
+  std::vector<double> load(nlanes, 0.0);
+  std::vector<char> used(nlanes, 0);
+  if (nlanes > 1) {
+    CUDA_OK(cudaEventRecord(c->ev_fork, st));
+    for (int l = 1; l < nlanes; ++l) CUDA_OK(cudaStreamWaitEvent(c->side[l - 1], c->ev_fork, 0));
+  }
+  for (size_t s : order) {
+    const int lane = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[lane] += w->cost[s];
+    used[lane] = 1;
+    const cudaStream_t ls = lane == 0 ? st : c->side[lane - 1];
     const int v = w->kernel[s];
-    const bool f32 = v >= sqb::kNumClassKernels;
-    const int kidx = f32 ? v - sqb::kNumClassKernels : v;
-    const sqb::ClassKernel& K = sqb::kClassKernels[kidx];
-    const PairClass& B = c->cls[K.bra_cls];
-    const PairClass& T = c->cls[K.ket_cls];
-    sqb::JKArgs a;
-    memset(&a, 0, sizeof(a));
-    a.bra_pairs = B.d_pairs; a.bra_prims = B.d_prims;
-    a.ket_pairs = T.d_pairs; a.ket_prims = T.d_prims;
-    a.PA = dPA; a.PB = dPB; a.PT = c->d_PT; a.PM = c->d_PM;
-    a.Jacc = c->d_J; a.KAacc = c->d_KA; a.KBacc = c->d_KB;
-    a.boys_tab = c->d_boys;
-    a.counters = c->d_counters + 4 * v;
-    a.bra_prims_f = B.d_primsf; a.ket_prims_f = T.d_primsf;
-    a.nbf = n; a.ns = c->ns;
-    a.same_class = K.bra_cls == K.ket_cls;
-    a.cut_outer = outer; a.cut_fixed = fixed; a.dscreen_rmax = dscreen;
-    const sqb::WorkItem* items = w->d_items + w->first[s];
-    void* args[] = {&a, &items};
-    const bool ws = !f32 && c->use_ws && K.ws_r != nullptr;
-    if (!f32) c->ran_ws[kidx] = ws;
-    const size_t smem = (size_t)B.max_nprim * B.stride * (f32 ? sizeof(float) : sizeof(double)) +
-                        (ws ? (size_t)K.ws_warps * K.ws_nr * 32 * sizeof(double) : 0);
-    const void* fn = f32 ? (uhf ? K.fn_u32 : K.fn_r32) : ws ? (uhf ? K.ws_u : K.ws_r) : (uhf ? K.fn_u : K.fn_r);
-    const dim3 grid(w->count[s], ws ? 1 : (f32 ? K.passes32 : K.passes)), block(ws ? 32 * K.ws_warps : 128);
-    if (smem > 48 * 1024) CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const SegLaunch L = seg_single(c, w, s, dPA, dPB, uhf, -1);
     sqb200_jk::Ev ev{v, nullptr, nullptr};
     if (c->profile) {
       CUDA_OK(cudaEventCreate(&ev.a));
       CUDA_OK(cudaEventCreate(&ev.b));
       CUDA_OK(cudaEventRecord(ev.a, st));
     }
-    CUDA_OK(cudaLaunchKernel(fn, grid, block, args, smem, st));
+    rc = enqueue(L, ls);
+    if (rc) return rc;
     if (c->profile) {
       CUDA_OK(cudaEventRecord(ev.b, st));
       c->events.push_back(ev);
     }
+  }
+  for (int l = 1; l < nlanes; ++l) {   // join (every forked lane, used or not, so st waits on all)
+    CUDA_OK(cudaEventRecord(c->ev_join[l - 1], c->side[l - 1]));
+    CUDA_OK(cudaStreamWaitEvent(st, c->ev_join[l - 1], 0));
   }
   k_finalize<<<grid_for(nn, 256), 256, 0, st>>>(c->d_J, c->d_KA, c->d_KB, dJT, dKA, dKB, n, uhf);
   CUDA_OK(cudaGetLastError());
@@ -743,16 +873,36 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
 }
 
 // Algorithmic FP64/FP32 operations of kernel index v (FP64 form v < K, FP32 form v - K)
-// from its four counters [quartets, primitive quartets, bra flushes, digestions].
+// from its four counters [quartets, primitive quartets, bra flushes, digestions]: per
+// primitive quartet the pass-free count (Boys function and R once), per flush and digestion
+// the operations of the form that ran (those are not repeated across passes).
 double kernel_flops(const sqb200_jk* c, int v, const unsigned long long* h) {
   const int K_ = sqb::kNumClassKernels;
   const bool f32 = v >= K_;
   const sqb::ClassKernel& K = sqb::kClassKernels[f32 ? v - K_ : v];
   const bool ws = !f32 && v < (int)c->ran_ws.size() && c->ran_ws[v];
-  const double fp = f32 ? K.f32_flops_prim : ws ? K.ws_flops_prim : K.flops_prim;
+  const double fp = K.alg_flops_prim;
   const double ff = f32 ? K.f32_flops_flush : ws ? K.ws_flops_flush : K.flops_flush;
   const double fq = f32 ? K.f32_flops_quartet : ws ? K.ws_flops_quartet : K.flops_quartet;
   return (double)h[1] * fp + (double)h[2] * ff + (double)h[3] * fq;
+}
+
+// Mean device time (ms) of `reps` launches of L on st after one untimed launch.
+int time_seg(const SegLaunch& L, cudaStream_t st, int reps, double* ms) {
+  cudaEvent_t a, b;
+  CUDA_OK(cudaEventCreate(&a));
+  CUDA_OK(cudaEventCreate(&b));
+  int rc = enqueue(L, st);
+  if (!rc) rc = cudaEventRecord(a, st) == cudaSuccess ? SQB200_OK : fail(SQB200_ECUDA, "cudaEventRecord");
+  for (int r = 0; r < reps && !rc; ++r) rc = enqueue(L, st);
+  if (!rc) rc = cudaEventRecord(b, st) == cudaSuccess ? SQB200_OK : fail(SQB200_ECUDA, "cudaEventRecord");
+  float t = 0.f;
+  if (!rc) rc = cudaEventSynchronize(b) == cudaSuccess ? SQB200_OK : fail(SQB200_ECUDA, "cudaEventSynchronize");
+  if (!rc) rc = cudaEventElapsedTime(&t, a, b) == cudaSuccess ? SQB200_OK : fail(SQB200_ECUDA, "cudaEventElapsedTime");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = t / reps;
+  return rc;
 }
 
 }  // namespace
@@ -776,6 +926,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   const char* ws_env = getenv("SQB200_WS");
   c->use_ws = !(ws_env && ws_env[0] == '0');
   c->ran_ws.assign(sqb::kNumClassKernels, 0);
+  c->wide.assign(sqb::kNumClassKernels, 0);
   c->nbf = nbf;
   int rc = build_shells(nbf, nprim, lmn, xyz, exps, ncoefs, c->shells);
   if (rc) { delete c; return rc; }
@@ -804,6 +955,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   ALLOC(c->d_KAo, nn * sizeof(double));
   ALLOC(c->d_KBo, nn * sizeof(double));
   ALLOC(c->d_counters, 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
+  ALLOC(c->d_mol, sizeof(sqb::MolRec));
 #undef ALLOC
   cudaError_t e = cudaMemcpy(c->d_boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(c->d_shfirst, fst.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
@@ -827,14 +979,60 @@ int sqb200_jk_destroy(sqb200_jk* c) {
   if (!c) return SQB200_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (size_t i = 0; i < c->side.size(); ++i) {
+    cudaStreamSynchronize(c->side[i]);
+    cudaStreamDestroy(c->side[i]);
+    cudaEventDestroy(c->ev_join[i]);
+  }
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   for (auto& kv : c->work) cudaFree(kv.second.d_items);
   for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   free_pairs(c);
   void* ptrs[] = {c->d_boys, c->d_shfirst, c->d_shn, c->d_PA, c->d_PB, c->d_PT, c->d_PM, c->d_J, c->d_KA,
-                  c->d_KB, c->d_JT, c->d_KAo, c->d_KBo, c->d_counters};
+                  c->d_KB, c->d_JT, c->d_KAo, c->d_KBo, c->d_counters, c->d_mol};
   for (void* p : ptrs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+  return SQB200_OK;
+}
+
+int sqb200_jk_autotune(sqb200_jk* c, const double* dPA, const double* dPB, int restricted, double outer,
+                       double fixed, double dscreen, void* stream) {
+  if (!c || !dPA) return fail(SQB200_EINVAL, "null argument");
+  CUDA_OK(cudaSetDevice(c->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const int uhf = restricted ? 0 : 1;
+  if (dPB == nullptr) dPB = dPA;
+  sqb200_jk::Work* w = nullptr;
+  int rc = build_work(c, outer, fixed, &w);
+  if (rc) return rc;
+  // the class kernels read PT, PM and the molecule record: set them up as a build does
+  const int n = c->nbf, nn = n * n;
+  const sqb::MolRec mv{0, 0, n, c->ns, outer, fixed, dscreen, 0, uhf};
+  k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf, c->d_mol, mv);
+  k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM);
+  for (size_t s = 0; s < w->kernel.size(); ++s) {
+    const int v = w->kernel[s];
+    if (v >= sqb::kNumClassKernels || !sqb::kClassKernels[v].fn_rw) continue;
+    double tn = 0.0, tw = 0.0;
+    rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, 0), st, 2, &tn);
+    if (!rc) rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, 1), st, 2, &tw);
+    if (rc) return rc;
+    c->wide[v] = tw < tn ? 1 : 0;
+  }
+  CUDA_OK(cudaStreamSynchronize(st));
+  return SQB200_OK;
+}
+
+int sqb200_jk_tiles(sqb200_jk* c, int* wide, int n) {
+  if (!c || !wide) return fail(SQB200_EINVAL, "null argument");
+  for (int k = 0; k < n && k < sqb::kNumClassKernels; ++k) wide[k] = sqb::kClassKernels[k].fn_rw ? c->wide[k] : -1;
+  return std::min(n, sqb::kNumClassKernels);
+}
+
+int sqb200_jk_set_tiles(sqb200_jk* c, const int* wide, int n) {
+  if (!c || !wide) return fail(SQB200_EINVAL, "null argument");
+  for (int k = 0; k < n && k < sqb::kNumClassKernels; ++k) c->wide[k] = wide[k] > 0 ? 1 : 0;
   return SQB200_OK;
 }
 
@@ -1012,7 +1210,8 @@ constexpr int kNoAllocMaxKernels = 64;
 constexpr size_t kNoAllocMat = (size_t)kNoAllocMaxNbf * kNoAllocMaxNbf;          // doubles per matrix
 constexpr size_t kNoAllocCountersOff = 5 * kNoAllocMat * sizeof(double);            // PT PM J KA KB
 constexpr size_t kNoAllocItemsOff = kNoAllocCountersOff + 4 * kNoAllocMaxKernels * sizeof(unsigned long long);
-constexpr size_t kNoAllocBytes = kNoAllocItemsOff + (size_t)kNoAllocMaxItems * sizeof(sqb::WorkItem);
+constexpr size_t kNoAllocMolOff = (kNoAllocItemsOff + (size_t)kNoAllocMaxItems * sizeof(sqb::WorkItem) + 255) / 256 * 256;
+constexpr size_t kNoAllocBytes = kNoAllocMolOff + 256;   // one molecule record
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -1065,7 +1264,7 @@ void noalloc_items(const sqb200_jk* c, double outer, double fixed, std::vector<s
             if (T.pairs[mid].schwarz >= thr) lo = mid + 1; else hi = mid;
           }
           const int start = (same && sx == sy) ? b : k0s;
-          for (int k0 = start; k0 < lo; k0 += kper) items.push_back({b, k0, std::min(kper, lo - k0), isplit});
+          for (int k0 = start; k0 < lo; k0 += kper) items.push_back({b, k0, std::min(kper, lo - k0), isplit, 0});
         }
       }
     if ((int)items.size() > f0) {
@@ -1110,7 +1309,9 @@ extern "C" int sqb200_jk_build_noalloc(sqb200_jk* c, const double* dPA, const do
   if (!items.empty())
     CUDA_OK(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(sqb::WorkItem), cudaMemcpyHostToDevice, st));
   // k_prep zeroes J, KA (and KB when unrestricted); the counters are cleared here
-  k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, PT, J, KA, KB, nn, uhf);
+  sqb::MolRec* d_mol = (sqb::MolRec*)(base + kNoAllocMolOff);
+  const sqb::MolRec mv{0, 0, n, c->ns, outer, fixed, dscreen, 0, uhf};
+  k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, PT, J, KA, KB, nn, uhf, d_mol, mv);
   k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, PT, c->d_shfirst, c->d_shn, c->ns, n, PM);
   CUDA_OK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 4 * sqb::kNumClassKernels, st));
   for (size_t s = 0; s < kernel.size(); ++s) {
@@ -1125,14 +1326,14 @@ extern "C" int sqb200_jk_build_noalloc(sqb200_jk* c, const double* dPA, const do
     a.Jacc = J; a.KAacc = KA; a.KBacc = KB;
     a.boys_tab = c->d_boys;
     a.counters = counters + 4 * kernel[s];
-    a.nbf = n; a.ns = c->ns;
+    a.mols = d_mol;
     a.same_class = K.bra_cls == K.ket_cls;
-    a.cut_outer = outer; a.cut_fixed = fixed; a.dscreen_rmax = dscreen;
     const sqb::WorkItem* it = d_items + first[s];
     void* args[] = {&a, &it};
     const size_t smem = (size_t)B.max_nprim * B.stride * sizeof(double);
     const void* fn = uhf ? K.fn_u : K.fn_r;
-    if (smem > 48 * 1024) CUDA_OK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int rs = ensure_smem(fn, smem);
+    if (rs) return rs;
     CUDA_OK(cudaLaunchKernel(fn, dim3(count[s], K.passes), dim3(128), args, smem, st));
   }
   k_finalize<<<grid_for(nn, 256), 256, 0, st>>>(J, KA, KB, dJT, dKA, dKB, n, uhf);
@@ -1194,5 +1395,395 @@ extern "C" int sqb200_oneint(sqb200_jk* c, int natom, const double* Z, const dou
   void* ptrs[] = {d_np, d_off, d_lmn, d_xyz, d_ex, d_nc, d_Z, d_A, d_out};
   for (void* q : ptrs) cudaFree(q);
   if (e != cudaSuccess) return fail(SQB200_ECUDA, std::string("sqb200_oneint: ") + cudaGetErrorString(e));
+  return SQB200_OK;
+}
+
+// ---------------------------------------------------------------- batched builds
+//
+// A batch joins the contexts of many molecules (each created by sqb200_jk_create) into one set
+// of merged class arrays, so that one launch per class kernel carries the work items of every
+// molecule.  Densities and outputs are packed: molecule m's nbf_m x nbf_m block starts at
+// offset off[m] of every array.  Pair records keep molecule-local shell and function indices;
+// each work item names its molecule, whose MolRec gives the matrix offsets and cutoffs.
+
+struct sqb200_batch {
+  int device = 0, nmol = 0;
+  std::vector<sqb200_jk*> mols;
+  std::vector<long long> moff, pmoff;   // nmol + 1 entries
+  std::vector<int> shoff;               // nmol + 1 entries
+  int max_ns = 0, max_nbf = 0;
+  struct Cls {
+    std::vector<int> pair_base;         // per molecule: its first pair in the merged array
+    int max_nprim = 0, stride = 0;
+    sqb::PairRec* d_pairs = nullptr;
+    double* d_prims = nullptr;
+    float* d_primsf = nullptr;
+  } cls[sqb::kNumPairClasses];
+  std::vector<sqb::MolRec> rec;
+  sqb::MolRec* d_mols = nullptr;
+  int *d_shfirst = nullptr, *d_shn = nullptr;
+  double *d_PT = nullptr, *d_PM = nullptr, *d_J = nullptr, *d_KA = nullptr, *d_KB = nullptr;
+  unsigned long long* d_counters = nullptr;   // 4 per kernel form and spin: [spin][2K][4]
+  // work list of the current step: segments per (class kernel form, spin)
+  std::vector<int> kernel, spin, first, count;
+  std::vector<double> cost;
+  sqb::WorkItem* d_items = nullptr;
+  size_t items_cap = 0;
+  bool have_step = false;
+  std::vector<unsigned long long> last_counts;
+  std::vector<char> wide;               // per class kernel: wide-tile FP64 form (sqb200_batch_autotune)
+  int last_launches = 0;
+  int nside = -1;
+  std::vector<cudaStream_t> side;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+// PM blocks of every molecule of a batch: grid.y = molecule
+__global__ void k_pmax_batch(const double* __restrict__ PA, const double* __restrict__ PB,
+                             const double* __restrict__ PT, const int* __restrict__ first,
+                             const int* __restrict__ nf, const sqb::MolRec* __restrict__ mols,
+                             double* __restrict__ PM) {
+  const sqb::MolRec mr = mols[blockIdx.y];
+  const int ns = mr.ns, n = mr.nbf;
+  const int* f = first + mr.shoff;
+  const int* c = nf + mr.shoff;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ns * ns; idx += gridDim.x * blockDim.x) {
+    const int P = idx / ns, Q = idx % ns;
+    double r = 0.0;
+    for (int p = 0; p < c[P]; ++p)
+      for (int q = 0; q < c[Q]; ++q) {
+        const long long o = mr.moff + (long long)(f[P] + p) * n + f[Q] + q;
+        r = fmax(r, fabs(PT[o]));
+        r = fmax(r, fabs(PA[o]));
+        r = fmax(r, fabs(PB[o]));
+      }
+    PM[mr.pmoff + idx] = r;
+  }
+}
+
+// per-molecule symmetrisation of a batch: JT = J + J^T, KA = -(K + K^T), KB likewise or = KA
+__global__ void k_finalize_batch(const double* __restrict__ J, const double* __restrict__ KA,
+                                 const double* __restrict__ KB, double* __restrict__ JT,
+                                 double* __restrict__ KAo, double* __restrict__ KBo,
+                                 const sqb::MolRec* __restrict__ mols) {
+  const sqb::MolRec mr = mols[blockIdx.y];
+  const int n = mr.nbf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x) {
+    const int r = i / n, c = i % n;
+    const long long a = mr.moff + i, t = mr.moff + (long long)c * n + r;
+    JT[a] = J[a] + J[t];
+    const double ka = -(KA[a] + KA[t]);
+    KAo[a] = ka;
+    KBo[a] = mr.uhf ? -(KB[a] + KB[t]) : ka;
+  }
+}
+
+void free_batch(sqb200_batch* b) {
+  for (size_t i = 0; i < b->side.size(); ++i) {
+    cudaStreamSynchronize(b->side[i]);
+    cudaStreamDestroy(b->side[i]);
+    cudaEventDestroy(b->ev_join[i]);
+  }
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->stream) { cudaStreamSynchronize(b->stream); cudaStreamDestroy(b->stream); }
+  for (auto& k : b->cls) { cudaFree(k.d_pairs); cudaFree(k.d_prims); cudaFree(k.d_primsf); }
+  void* ptrs[] = {b->d_mols, b->d_shfirst, b->d_shn, b->d_PT, b->d_PM, b->d_J, b->d_KA, b->d_KB,
+                  b->d_counters, b->d_items};
+  for (void* p : ptrs) cudaFree(p);
+  delete b;
+}
+
+}  // namespace
+
+extern "C" int sqb200_batch_create(sqb200_batch** out, int nmol, sqb200_jk* const* mols) {
+  if (!out || nmol <= 0 || !mols) return fail(SQB200_EINVAL, "sqb200_batch_create: null argument or nmol <= 0");
+  if (nmol > 65535) return fail(SQB200_EINVAL, "sqb200_batch_create: at most 65535 molecules per batch");
+  *out = nullptr;
+  for (int m = 0; m < nmol; ++m) {
+    if (!mols[m]) return fail(SQB200_EINVAL, "sqb200_batch_create: null context");
+    if (mols[m]->device != mols[0]->device) return fail(SQB200_EINVAL, "sqb200_batch_create: contexts on different devices");
+  }
+  sqb200_batch* b = new sqb200_batch();
+  b->device = mols[0]->device;
+  b->nmol = nmol;
+  b->mols.assign(mols, mols + nmol);
+  b->moff.assign(nmol + 1, 0);
+  b->pmoff.assign(nmol + 1, 0);
+  b->shoff.assign(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) {
+    const sqb200_jk* c = mols[m];
+    b->moff[m + 1] = b->moff[m] + (long long)c->nbf * c->nbf;
+    b->pmoff[m + 1] = b->pmoff[m] + (long long)c->ns * c->ns;
+    b->shoff[m + 1] = b->shoff[m] + c->ns;
+    b->max_ns = std::max(b->max_ns, c->ns);
+    b->max_nbf = std::max(b->max_nbf, c->nbf);
+  }
+  cudaError_t e = cudaSetDevice(b->device);
+  auto bail = [&](int code, const std::string& msg) { free_batch(b); return fail(code, "sqb200_batch_create: " + msg); };
+  if (e != cudaSuccess) return bail(SQB200_ECUDA, cudaGetErrorString(e));
+  // merged class arrays
+  for (int k = 0; k < sqb::kNumPairClasses; ++k) {
+    auto& bc = b->cls[k];
+    std::vector<sqb::PairRec> pairs;
+    std::vector<double> prims;
+    bc.pair_base.assign(nmol, 0);
+    for (int m = 0; m < nmol; ++m) {
+      const PairClass& pc = mols[m]->cls[k];
+      bc.pair_base[m] = (int)pairs.size();
+      if (pc.pairs.empty()) continue;
+      const int pbase = (int)prims.size();
+      for (sqb::PairRec r : pc.pairs) { r.poff += pbase; pairs.push_back(r); }
+      prims.insert(prims.end(), pc.prims.begin(), pc.prims.end());
+      bc.max_nprim = std::max(bc.max_nprim, pc.max_nprim);
+      bc.stride = pc.stride;
+    }
+    if (pairs.empty()) continue;
+    if (prims.size() >= (size_t)INT_MAX) return bail(SQB200_EINVAL, "merged primitive array exceeds 2^31 entries");
+    std::vector<float> pf(prims.begin(), prims.end());
+    e = cudaMalloc(&bc.d_pairs, pairs.size() * sizeof(sqb::PairRec));
+    if (e == cudaSuccess) e = cudaMalloc(&bc.d_prims, prims.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&bc.d_primsf, pf.size() * sizeof(float));
+    if (e != cudaSuccess) return bail(SQB200_ENOMEM, cudaGetErrorString(e));
+    e = cudaMemcpy(bc.d_pairs, pairs.data(), pairs.size() * sizeof(sqb::PairRec), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bc.d_prims, prims.data(), prims.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(bc.d_primsf, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return bail(SQB200_ECUDA, cudaGetErrorString(e));
+  }
+  // packed shell tables and per-molecule buffers
+  std::vector<int> fst, nf;
+  for (int m = 0; m < nmol; ++m)
+    for (const Shell& sh : mols[m]->shells) { fst.push_back(sh.first); nf.push_back(sh.nfunc); }
+  const size_t ntot = (size_t)b->moff[nmol], pmtot = (size_t)b->pmoff[nmol];
+  e = cudaMalloc(&b->d_mols, nmol * sizeof(sqb::MolRec));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_shfirst, fst.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_shn, nf.size() * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_PT, ntot * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_PM, pmtot * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_J, ntot * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_KA, ntot * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_KB, ntot * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 2 * 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
+  if (e != cudaSuccess) return bail(SQB200_ENOMEM, cudaGetErrorString(e));
+  e = cudaMemcpy(b->d_shfirst, fst.data(), fst.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_shn, nf.data(), nf.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(SQB200_ECUDA, cudaGetErrorString(e));
+  b->wide.assign(sqb::kNumClassKernels, 0);
+  b->rec.resize(nmol);
+  for (int m = 0; m < nmol; ++m)
+    b->rec[m] = sqb::MolRec{b->moff[m], b->pmoff[m], mols[m]->nbf, mols[m]->ns, 0.0, 0.0, 0.0, b->shoff[m], 0};
+  *out = b;
+  return SQB200_OK;
+}
+
+extern "C" int sqb200_batch_destroy(sqb200_batch* b) {
+  if (!b) return SQB200_OK;
+  cudaSetDevice(b->device);
+  free_batch(b);
+  return SQB200_OK;
+}
+
+extern "C" int sqb200_batch_offsets(sqb200_batch* b, long long* off) {
+  if (!b || !off) return fail(SQB200_EINVAL, "null argument");
+  for (int m = 0; m <= b->nmol; ++m) off[m] = b->moff[m];
+  return SQB200_OK;
+}
+
+extern "C" int sqb200_batch_set_step(sqb200_batch* b, const int* restricted, const double* scf_cutoff,
+                                     const double* fixed_cutoff, const double* dscreen_rmax) {
+  if (!b || !restricted || !scf_cutoff || !fixed_cutoff || !dscreen_rmax) return fail(SQB200_EINVAL, "null argument");
+  CUDA_OK(cudaSetDevice(b->device));
+  // the work list depends on the spins and the two Schwarz cutoffs (and each context's FP32
+  // threshold); the density-screen bound only reaches the kernels through the records
+  bool same = b->have_step;
+  for (int m = 0; m < b->nmol && same; ++m)
+    same = b->rec[m].uhf == (restricted[m] ? 0 : 1) && b->rec[m].cut_outer == scf_cutoff[m] &&
+           b->rec[m].cut_fixed == fixed_cutoff[m];
+  for (int m = 0; m < b->nmol; ++m) {
+    b->rec[m].uhf = restricted[m] ? 0 : 1;
+    b->rec[m].cut_outer = scf_cutoff[m];
+    b->rec[m].cut_fixed = fixed_cutoff[m];
+    b->rec[m].dscreen_rmax = dscreen_rmax[m];
+  }
+  CUDA_OK(cudaStreamSynchronize(b->stream));
+  for (cudaStream_t s : b->side) CUDA_OK(cudaStreamSynchronize(s));
+  CUDA_OK(cudaMemcpy(b->d_mols, b->rec.data(), b->nmol * sizeof(sqb::MolRec), cudaMemcpyHostToDevice));
+  if (same) return SQB200_OK;
+  b->kernel.clear(); b->spin.clear(); b->first.clear(); b->count.clear(); b->cost.clear();
+  std::vector<sqb::WorkItem> items, items32;
+  const int K_ = sqb::kNumClassKernels;
+  for (int sp = 0; sp < 2; ++sp)
+    for (int ki = 0; ki < K_; ++ki) {
+      const sqb::ClassKernel& K = sqb::kClassKernels[ki];
+      const int f64 = (int)items.size();
+      items32.clear();
+      double c64 = 0.0, c32 = 0.0;
+      for (int m = 0; m < b->nmol; ++m) {
+        if (b->rec[m].uhf != sp) continue;
+        class_items(b->mols[m], ki, scf_cutoff[m], fixed_cutoff[m], b->cls[K.bra_cls].pair_base[m],
+                    b->cls[K.ket_cls].pair_base[m], m, items, items32, c64, c32);
+      }
+      if ((int)items.size() > f64) {
+        b->kernel.push_back(ki); b->spin.push_back(sp); b->first.push_back(f64);
+        b->count.push_back((int)items.size() - f64); b->cost.push_back(c64);
+      }
+      if (!items32.empty()) {
+        b->kernel.push_back(ki + K_); b->spin.push_back(sp); b->first.push_back((int)items.size());
+        b->count.push_back((int)items32.size()); b->cost.push_back(c32);
+        items.insert(items.end(), items32.begin(), items32.end());
+      }
+    }
+  for (int c : b->count)
+    if (c > 2147483647 / 2) return fail(SQB200_EINVAL, "sqb200_batch_set_step: too many work items in one class");
+  if (items.size() > b->items_cap) {
+    cudaFree(b->d_items);
+    b->d_items = nullptr;
+    b->items_cap = 0;
+    CUDA_OK(cudaMalloc(&b->d_items, items.size() * sizeof(sqb::WorkItem)));
+    b->items_cap = items.size();
+  }
+  if (!items.empty())
+    CUDA_OK(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(sqb::WorkItem), cudaMemcpyHostToDevice));
+  b->have_step = true;
+  return SQB200_OK;
+}
+
+// Segment s of a batch's work list; wide < 0 takes the batch's tile choice.
+SegLaunch seg_batch(sqb200_batch* b, size_t s, const double* dPA, const double* dPB, int wide) {
+  SegLaunch L;
+  const int K_ = sqb::kNumClassKernels;
+  const int v = b->kernel[s], uhf = b->spin[s];
+  const bool f32 = v >= K_;
+  const int kidx = f32 ? v - K_ : v;
+  const sqb::ClassKernel& K = sqb::kClassKernels[kidx];
+  const auto& B = b->cls[K.bra_cls];
+  const auto& T = b->cls[K.ket_cls];
+  sqb::JKArgs& a = L.a;
+  memset(&a, 0, sizeof(a));
+  a.bra_pairs = B.d_pairs; a.bra_prims = B.d_prims;
+  a.ket_pairs = T.d_pairs; a.ket_prims = T.d_prims;
+  a.bra_prims_f = B.d_primsf; a.ket_prims_f = T.d_primsf;
+  a.PA = dPA; a.PB = dPB; a.PT = b->d_PT; a.PM = b->d_PM;
+  a.Jacc = b->d_J; a.KAacc = b->d_KA; a.KBacc = b->d_KB;
+  a.boys_tab = b->mols[0]->d_boys;
+  a.counters = b->d_counters + 4 * (uhf * 2 * K_ + v);
+  a.mols = b->d_mols;
+  a.same_class = K.bra_cls == K.ket_cls;
+  L.items = b->d_items + b->first[s];
+  L.smem = (size_t)B.max_nprim * B.stride * (f32 ? sizeof(float) : sizeof(double));
+  int passes = 1;
+  pick_form(K, f32, uhf, wide < 0 ? (b->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
+  L.grid = dim3(b->count[s], passes);
+  L.block = dim3(128);
+  return L;
+}
+
+void batch_prologue(sqb200_batch* b, const double* dPA, const double* dPB, cudaStream_t st) {
+  const long long ntot = b->moff[b->nmol];
+  k_prep<<<grid_for(ntot, 256), 256, 0, st>>>(dPA, dPB, b->d_PT, b->d_J, b->d_KA, b->d_KB, (int)ntot, 1,
+                                              nullptr, sqb::MolRec{});
+  k_pmax_batch<<<dim3((b->max_ns * b->max_ns + 127) / 128, b->nmol), 128, 0, st>>>(
+      dPA, dPB, b->d_PT, b->d_shfirst, b->d_shn, b->d_mols, b->d_PM);
+}
+
+extern "C" int sqb200_batch_autotune(sqb200_batch* b, const double* dPA, const double* dPB, void* stream) {
+  if (!b || !dPA || !dPB) return fail(SQB200_EINVAL, "null argument");
+  if (!b->have_step) return fail(SQB200_EINVAL, "sqb200_batch_autotune: call sqb200_batch_set_step first");
+  CUDA_OK(cudaSetDevice(b->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  batch_prologue(b, dPA, dPB, st);
+  // a class with restricted and unrestricted segments keeps one choice: the summed time decides
+  std::vector<double> tn(sqb::kNumClassKernels, 0.0), tw(sqb::kNumClassKernels, 0.0);
+  for (size_t s = 0; s < b->kernel.size(); ++s) {
+    const int v = b->kernel[s];
+    if (v >= sqb::kNumClassKernels || !sqb::kClassKernels[v].fn_rw) continue;
+    double a = 0.0, w = 0.0;
+    int rc = time_seg(seg_batch(b, s, dPA, dPB, 0), st, 2, &a);
+    if (!rc) rc = time_seg(seg_batch(b, s, dPA, dPB, 1), st, 2, &w);
+    if (rc) return rc;
+    tn[v] += a;
+    tw[v] += w;
+  }
+  for (int k = 0; k < sqb::kNumClassKernels; ++k) b->wide[k] = (tw[k] > 0.0 && tw[k] < tn[k]) ? 1 : 0;
+  CUDA_OK(cudaStreamSynchronize(st));
+  return SQB200_OK;
+}
+
+extern "C" int sqb200_batch_build_device(sqb200_batch* b, const double* dPA, const double* dPB, double* dJT,
+                                         double* dKA, double* dKB, void* stream) {
+  if (!b || !dPA || !dPB || !dJT || !dKA || !dKB) return fail(SQB200_EINVAL, "null argument");
+  if (!b->have_step) return fail(SQB200_EINVAL, "sqb200_batch_build_device: call sqb200_batch_set_step first");
+  CUDA_OK(cudaSetDevice(b->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
+  const int K_ = sqb::kNumClassKernels;
+  batch_prologue(b, dPA, dPB, st);
+  CUDA_OK(cudaMemsetAsync(b->d_counters, 0, 2 * 8 * K_ * sizeof(unsigned long long), st));
+  if (b->nside < 0) {
+    int n = 4;
+    if (const char* e = getenv("SQB200_STREAMS")) n = std::max(0, std::min(16, atoi(e)));
+    CUDA_OK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    for (int i = 0; i < n; ++i) {
+      cudaStream_t s;
+      cudaEvent_t e;
+      CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      b->side.push_back(s);
+      b->ev_join.push_back(e);
+    }
+    b->nside = n;
+  }
+  const int nlanes = 1 + b->nside;
+  std::vector<size_t> order(b->kernel.size());
+  for (size_t s = 0; s < order.size(); ++s) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) { return b->cost[x] > b->cost[y]; });
+  std::vector<double> load(nlanes, 0.0);
+  if (nlanes > 1) {
+    CUDA_OK(cudaEventRecord(b->ev_fork, st));
+    for (int l = 1; l < nlanes; ++l) CUDA_OK(cudaStreamWaitEvent(b->side[l - 1], b->ev_fork, 0));
+  }
+  for (size_t s : order) {
+    const int lane = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[lane] += b->cost[s];
+    const cudaStream_t ls = lane == 0 ? st : b->side[lane - 1];
+    const int rc = enqueue(seg_batch(b, s, dPA, dPB, -1), ls);
+    if (rc) return rc;
+  }
+  for (int l = 1; l < nlanes; ++l) {
+    CUDA_OK(cudaEventRecord(b->ev_join[l - 1], b->side[l - 1]));
+    CUDA_OK(cudaStreamWaitEvent(st, b->ev_join[l - 1], 0));
+  }
+  k_finalize_batch<<<dim3((b->max_nbf * b->max_nbf + 255) / 256, b->nmol), 256, 0, st>>>(
+      b->d_J, b->d_KA, b->d_KB, dJT, dKA, dKB, b->d_mols);
+  CUDA_OK(cudaGetLastError());
+  b->last_launches = 3 + (int)b->kernel.size();
+  return SQB200_OK;
+}
+
+extern "C" int sqb200_batch_stats(sqb200_batch* b, long long* out, int n) {
+  if (!b || !out) return fail(SQB200_EINVAL, "null argument");
+  CUDA_OK(cudaSetDevice(b->device));
+  const int K_ = sqb::kNumClassKernels;
+  std::vector<unsigned long long> h(2 * 8 * K_);
+  CUDA_OK(cudaMemcpy(h.data(), b->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  long long q = 0, pq = 0;
+  double fl = 0.0;
+  for (int sp = 0; sp < 2; ++sp)
+    for (int v = 0; v < 2 * K_; ++v) {
+      const unsigned long long* c = &h[4 * (sp * 2 * K_ + v)];
+      q += (long long)c[0];
+      pq += (long long)c[1];
+      fl += kernel_flops(b->mols[0], v, c);
+    }
+  long long pairs = 0, shells = 0;
+  for (const sqb200_jk* c : b->mols) {
+    shells += c->ns;
+    for (int k = 0; k < sqb::kNumPairClasses; ++k) pairs += (long long)c->cls[k].pairs.size();
+  }
+  long long v[6] = {q, pq, (long long)fl, shells, pairs, (long long)b->last_launches};
+  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
   return SQB200_OK;
 }

@@ -15,7 +15,7 @@ struct ClassKernel {
   int passes;             // ket-function blocks = grid.y of a launch
   const void* fn_r;       // restricted kernel
   const void* fn_u;       // unrestricted kernel
-  int flops_prim;         // FP64 ops per primitive quartet (all passes)
+  int flops_prim;         // FP64 ops per primitive quartet as emitted (all passes, repeats included)
   int flops_flush;        // FP64 ops per bra primitive and ket pair (all passes)
   int flops_quartet;      // FP64 ops of one digestion (all passes) of a (partial) quartet block
   // warp-specialised form (null when the class has one pass or its R buffer does not fit):
@@ -30,6 +30,15 @@ struct ClassKernel {
   const void* fn_r32;
   const void* fn_u32;
   int f32_flops_prim, f32_flops_flush, f32_flops_quartet;
+  // algorithmic operations per primitive quartet (pass-free: the Boys function and every R
+  // value once); the work figure of the roofline, the same for every form of the class
+  int alg_flops_prim;
+  // wide-tile FP64 form (fewer passes of more ket functions each); null when it would not
+  // merge any pass.  sqb200_jk_autotune picks the faster form per class.
+  int passes_w;
+  const void* fn_rw;
+  const void* fn_uw;
+  int w_flops_prim, w_flops_flush, w_flops_quartet;
 };
 
 extern const ClassKernel kClassKernels[];

@@ -23,7 +23,9 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_jk_build_device",
            "sqb200_jk_stats", "sqb200_jk_profile", "sqb200_jk_profile_read", "sqb200_jk_class_name",
            "sqb200_jk_schwarz", "sqb200_jk_mem_cutoff", "sqb200_jk_set_precision", "sqb200_oneint",
-           "sqb200_peak_fma",
+           "sqb200_peak_fma", "sqb200_batch_create", "sqb200_batch_destroy", "sqb200_batch_offsets",
+           "sqb200_batch_set_step", "sqb200_batch_build_device", "sqb200_batch_stats",
+           "sqb200_batch_autotune", "sqb200_jk_autotune", "sqb200_jk_tiles", "sqb200_jk_set_tiles",
            "sqb200_last_error"]
 
 
@@ -57,6 +59,17 @@ def load_library(path=LIB_PATH):
     L.sqb200_oneint.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
     L.sqb200_peak_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(ctypes.c_double)]
+    L.sqb200_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+    L.sqb200_batch_destroy.argtypes = [vp]
+    L.sqb200_batch_offsets.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.sqb200_batch_set_step.argtypes = [vp, _i32p, _f64p, _f64p, _f64p]
+    L.sqb200_batch_build_device.argtypes = [vp, vp, vp, vp, vp, vp, vp]
+    L.sqb200_batch_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    L.sqb200_batch_autotune.argtypes = [vp, vp, vp, vp]
+    L.sqb200_jk_autotune.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, vp]
+    L.sqb200_jk_tiles.argtypes = [vp, _i32p, ctypes.c_int]
+    L.sqb200_jk_set_tiles.argtypes = [vp, _i32p, ctypes.c_int]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.sqb200_last_error.restype = ctypes.c_char_p
@@ -146,6 +159,27 @@ class JKEngine:
         if legacy:
             self.stats()                           # synchronises the context stream
 
+    def autotune(self, dPA, dPB=None, restricted=True, scf_cutoff=1e-10, fixed_cutoff=None,
+                 dscreen_rmax=float("inf"), stream=None):
+        """Time the narrow and wide tile forms of every multi-pass class on this density's work
+        list and keep the faster per class (device pointers; synchronous)."""
+        if fixed_cutoff is None:
+            fixed_cutoff = scf_cutoff
+        _check(_lib.sqb200_jk_autotune(self._ctx, dPA, dPA if dPB is None else dPB, int(bool(restricted)),
+                                       scf_cutoff, fixed_cutoff, dscreen_rmax, stream))
+
+    def tiles(self):
+        """Per class kernel: 1 wide tile, 0 narrow tile, -1 single form."""
+        out = np.zeros(256, np.int32)
+        n = _lib.sqb200_jk_tiles(self._ctx, out, len(out))
+        if n < 0:
+            _check(n)
+        return out[:n].copy()
+
+    def set_tiles(self, wide):
+        w = np.ascontiguousarray(wide, dtype=np.int32)
+        _check(_lib.sqb200_jk_set_tiles(self._ctx, w, len(w)))
+
     def stats(self):
         """dict of the last build's counters."""
         out = (ctypes.c_longlong * 6)()
@@ -200,3 +234,57 @@ def peak_fma(device=0, iters=4096):
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(L.sqb200_peak_fma(device, iters, ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+class JKBatch:
+    """Batched J/K builds of many molecules (sqb200_batch_*): one launch per class kernel
+    carries every molecule's work.  `engines` are JKEngine contexts (kept alive by the batch).
+    Matrices are packed: molecule m's (nbf_m, nbf_m) block starts at element offsets[m]."""
+
+    def __init__(self, engines):
+        L = load_library()
+        self.engines = list(engines)
+        self.nmol = len(self.engines)
+        self._b = ctypes.c_void_p()
+        arr = (ctypes.c_void_p * self.nmol)(*[e._ctx.value for e in self.engines])
+        _check(L.sqb200_batch_create(ctypes.byref(self._b), self.nmol, arr))
+        off = (ctypes.c_longlong * (self.nmol + 1))()
+        _check(L.sqb200_batch_offsets(self._b, off))
+        self.offsets = [int(x) for x in off]
+        self.total = self.offsets[-1]
+
+    def set_step(self, restricted, scf_cutoff, fixed_cutoff=None, dscreen_rmax=None):
+        """Per-molecule spin flags and cutoffs (sequences of nmol; scalars broadcast)."""
+        def vec(x, dt):
+            a = np.broadcast_to(np.asarray(x, dtype=dt), (self.nmol,))
+            return np.ascontiguousarray(a)
+        fixed_cutoff = scf_cutoff if fixed_cutoff is None else fixed_cutoff
+        dscreen_rmax = float("inf") if dscreen_rmax is None else dscreen_rmax
+        _check(_lib.sqb200_batch_set_step(self._b, vec([1 if r else 0 for r in np.broadcast_to(
+            np.asarray(restricted), (self.nmol,))], np.int32), vec(scf_cutoff, np.float64),
+            vec(fixed_cutoff, np.float64), vec(dscreen_rmax, np.float64)))
+
+    def build_device(self, dPA, dPB, dJT, dKA, dKB, stream=None):
+        """Packed device pointers in and out; asynchronous on `stream` (a cudaStream_t handle)."""
+        _check(_lib.sqb200_batch_build_device(self._b, dPA, dPB, dJT, dKA, dKB, stream))
+
+    def autotune(self, dPA, dPB, stream=None):
+        """Tile autotuner over the batch's current work list (after set_step; synchronous)."""
+        _check(_lib.sqb200_batch_autotune(self._b, dPA, dPB, stream))
+
+    def stats(self):
+        out = (ctypes.c_longlong * 6)()
+        _check(_lib.sqb200_batch_stats(self._b, out, 6))
+        return {"quartets": out[0], "prim_quartets": out[1], "flops": out[2], "shells": out[3],
+                "pairs": out[4], "launches": out[5]}
+
+    def close(self):
+        if self._b:
+            _lib.sqb200_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
