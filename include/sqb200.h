@@ -171,6 +171,14 @@ int sqb200_batch_autotune(sqb200_batch *batch, const double *dPA, const double *
  * Synchronises with the device. */
 int sqb200_batch_stats(sqb200_batch *batch, long long *out, int n);
 
+/* Eigenvalues (ascending, W: batch x n) and eigenvectors of `batch` symmetric n x n FP64
+ * matrices stored back to back in A (device memory), in one cusolverDnXsyevBatched call on
+ * `stream`.  On return eigenvector k of matrix b is row k of A's b-th block (A read row-major).
+ * The SCF tail's eigensolve for many molecules of one padded size (in place of the
+ * reference's gen_sym_SomeEigen, src/lin.c:195, per molecule).  Asynchronous; grows a
+ * per-device workspace when needed (synchronising the device then). */
+int sqb200_syev_batched(int device, int n, int batch, double *A, double *W, void *stream);
+
 /* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,
  * src/matrix.c:389-440), written to the host array S (nbf*nbf). */
 int sqb200_jk_schwarz(sqb200_jk *ctx, double *S);

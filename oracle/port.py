@@ -114,6 +114,11 @@ def ref_run(args, timeout=3600):
             for kv in line.split()[1:]:
                 k, v = kv.split("=")
                 res[k] = float(v)
+    # SCF iteration lines of uhf() (src/uhf.c:1733: " %5d %20.8f %20.4E")
+    its = [t for t in (ln.split() for ln in r.stdout.splitlines())
+           if len(t) == 3 and t[0].isdigit() and "E" in t[2]]
+    if its:
+        res["iters"] = int(its[-1][0])
     return res
 
 

@@ -4,12 +4,13 @@ of independent molecules at once).
 Every molecule's J/K comes from ONE batched Fock build per iteration (sqb200_batch_*: one
 launch per class kernel over the work of all molecules), captured once as a CUDA graph and
 replayed each iteration.  The SCF tail runs batched as well: molecules are grouped into buckets
-of equal padded size (multiples of 32 functions); per bucket the Fock matrices, Pulay DIIS,
-orthogonalisation, cuSOLVER FP64 eigensolves and densities are stacked tensor operations.  A
-padded orbital gets a large diagonal shift so that it is never occupied.  Each molecule follows
-the same conventions and cutoff rule as scf.SCFJob (difference-density builds, 1STEP cutoff
-SCFConv / (nEA^2 + nEA nEB + nEB^2) / 50, first build without density screening above the
-memory cutoff), so each converged energy is the single-molecule result.
+of equal padded size (multiples of 32 functions); per bucket the Fock matrices,
+orthogonalisation, cuSOLVER FP64 eigensolves and densities are stacked tensor operations (a
+padded orbital gets a large diagonal shift so that it is never occupied), and the reference's
+density DIIS runs on the packed densities of all molecules at once.  Each molecule follows the
+loop, conventions and cutoff rule of scf.SCFJob (the reference's uhf() loop with its defaults:
+difference-density builds, 1STEP cutoff, conv_diis4, convergence on |dE| and the RMS density
+change); a molecule that has converged keeps its density while the others continue.
 
 Packed layout: molecule m's nbf_m x nbf_m block starts at offsets[m] of every packed array
 (the batch's layout); spin-resolved arrays hold the alpha blocks in [0, total) and the beta
@@ -22,8 +23,8 @@ import numpy as np
 
 from . import basis as B
 from . import molecules as M
-from .engine import JKBatch, JKEngine
-from .scf import electrons, nuclear_repulsion
+from .engine import JKBatch, JKEngine, syev_batched
+from .scf import SCF_MAX, DensityDIIS4, electrons, nuclear_repulsion
 
 PAD = 32            # bucket granularity (functions)
 SHIFT = 1.0e4       # Fock shift of padded orbitals (Eh): above every occupied level
@@ -45,6 +46,8 @@ class _Bucket:
             base = mo["off"] + s * total
             gi[r, :k, :k] = base + np.arange(k * k).reshape(k, k)
         self.gidx = torch.tensor(gi.reshape(-1), device=dev)
+        self.gidx2 = self.gidx.view(R, n * n)
+        self.mol_np = np.array([m for m, _ in rows], dtype=np.int64)
         valid = gi.reshape(-1) < 2 * total
         self.sidx = torch.tensor(gi.reshape(-1)[valid], device=dev)       # scatter targets
         self.svalid = torch.tensor(np.nonzero(valid)[0], device=dev)      # their stack positions
@@ -66,23 +69,21 @@ class _Bucket:
             S[r, :k, :k] = mols[m]["S"]
         self.X = torch.tensor(X, **f64)
         self.S = torch.tensor(S, **f64)
-        self.hF, self.hE = [], []             # DIIS history (stacked per iteration)
 
 
 class BatchSCF:
     """Solve many molecules together.  `jobs` is a list of dicts with keys atoms (angstrom),
     basis, and optionally charge, mult, restricted."""
 
-    def __init__(self, jobs, device=0, scf_conv=1e-8, fp32_below=0.0, diis_size=8, graph=True,
-                 autotune=True):
+    def __init__(self, jobs, device=0, scf_conv=1e-8, fp32_below=0.0, graph=True, autotune=True):
         import torch
         self.torch = torch
         self.dev = torch.device("cuda", device)
         self.stream = torch.cuda.Stream(self.dev)
         self.scf_conv = scf_conv
-        self.diis_size = diis_size
         self.use_graph = graph
         self.autotune = autotune
+        self._tuned = False
         self.mols = []
         self.engines = []
         t0 = time.perf_counter()
@@ -138,7 +139,11 @@ class BatchSCF:
                 Ph[T_ + o:T_ + o + k * k] = eye * (mo["nocc"][1] / tr)
             self.H.copy_(torch.tensor(Hh))
             self.P.copy_(torch.tensor(Ph))
+            self.P0 = self.P.clone()
             self.molid = torch.tensor(molid, device=self.dev)
+            self.molid2 = torch.cat([self.molid, self.molid])
+            self.nbf2 = torch.tensor([mo["nbf"] ** 2 for mo in self.mols], device=self.dev)
+            self.rmask = torch.tensor([mo["restricted"] for mo in self.mols], device=self.dev)[self.molid]
             self.enn = torch.tensor([mo["enn"] for mo in self.mols], **f64)
             # buckets of spin rows by padded size (restricted molecules: alpha row only)
             groups = {}
@@ -150,13 +155,31 @@ class BatchSCF:
         self.restricted = np.array([mo["restricted"] for mo in self.mols])
         self.energy = np.full(nm, np.nan)
         self.dE = np.full(nm, np.inf)
-        self.emax = np.full(nm, np.inf)
-        self.dPmax = np.full(nm, np.inf)
+        self.avgdP = np.full(nm, np.inf)
         self.converged = np.zeros(nm, dtype=bool)
+        self.iter_count = np.zeros(nm, dtype=np.int64)
         self.iters = 0
         self.graph = None
         self.first = True
         self.build_seconds = 0.0
+
+    def reset(self):
+        """Back to the identity-diagonal guess (same molecules, contexts, tiles and graph), so
+        that the same set can be solved again."""
+        T_ = self.total
+        with self.torch.cuda.stream(self.stream):
+            self.P.copy_(self.P0)
+            self.Pold.zero_()
+            self.K.zero_()
+            self.JT.zero_()
+        nm = len(self.mols)
+        self.energy = np.full(nm, np.nan)
+        self.dE = np.full(nm, np.inf)
+        self.avgdP = np.full(nm, np.inf)
+        self.converged = np.zeros(nm, dtype=bool)
+        self.iter_count = np.zeros(nm, dtype=np.int64)
+        self.iters = 0
+        self.first = True
 
     # ------------------------------------------------------------------ the Fock build
     def _build(self):
@@ -164,7 +187,7 @@ class BatchSCF:
         T_ = self.total
         P, dP = self.P, self.dP
         ptr = lambda t, k: t.data_ptr() + 8 * k
-        if self.graph is not None:
+        if self.graph is not None and not self.first:
             self.graph.replay()
             return
 
@@ -191,95 +214,103 @@ class BatchSCF:
 
     # ------------------------------------------------------------------ the SCF tail
     def _tail(self):
+        """One step of the reference's loop for every molecule (src/uhf.c:1600-1730): Fock from
+        the accumulated J/K, new densities from the lowest orbitals, their energy, conv_diis4.
+        Molecules that already met the convergence test keep their density (so their difference
+        density, and with it their share of the next builds, is zero)."""
         torch = self.torch
         T_ = self.total
         nm = len(self.mols)
-        # energies: E = Enn + sum PT.H + 1/2 sum PT.JT + 1/2 sum (PA.KA + PB.KB)
-        PA, PB = self.P[:T_], self.P[T_:2 * T_]
-        KA, KB = self.K[:T_], self.K[T_:2 * T_]
-        PT = PA + PB
-        dens = PT * (self.H + 0.5 * self.JT) + 0.5 * (PA * KA + PB * KB)
-        E = torch.zeros(nm, dtype=torch.float64, device=self.dev).index_add_(0, self.molid, dens) + self.enn
-        emax = torch.zeros(nm, dtype=torch.float64, device=self.dev)
-        self.Pold.copy_(self.P)
-        Fbase = torch.cat([self.H + self.JT, self.H + self.JT, torch.zeros(1, dtype=torch.float64, device=self.dev)])
-        Ffull = Fbase + self.K
-        newP = torch.zeros_like(self.P)
+        Fbase = self.H + self.JT
+        Ffull = torch.cat([Fbase, Fbase, torch.zeros(1, dtype=torch.float64, device=self.dev)]) + self.K
+        Pnew = torch.zeros_like(self.P)
         for b in self.buckets:
-            R, n = len(b.rows), b.n
-            F = Ffull[b.gidx].view(R, n, n)
-            D = self.P[b.gidx].view(R, n, n)
-            e = F @ D @ b.S
-            e = e - e.transpose(1, 2)
-            emax.scatter_reduce_(0, b.mol, e.abs().amax(dim=(1, 2)), reduce="amax")
-            # DIIS (common coefficients for the spin rows of one molecule)
-            b.hF.append(F)
-            b.hE.append(e)
-            if len(b.hF) > self.diis_size:
-                b.hF.pop(0)
-                b.hE.pop(0)
-            h = len(b.hF)
-            if h >= 2:
-                Es = torch.stack(b.hE, 1).reshape(R, h, -1)
-                Brow = Es @ Es.transpose(1, 2)                                  # (R, h, h)
-                Bm = torch.zeros((nm, h, h), dtype=torch.float64, device=self.dev).index_add_(0, b.mol, Brow)
-                Bm = Bm[b.mol]                                                   # back to rows
-                scale = Bm.diagonal(dim1=1, dim2=2).amax(dim=1).clamp_min(1e-300)
-                A = torch.zeros((R, h + 1, h + 1), dtype=torch.float64, device=self.dev)
-                A[:, :h, :h] = Bm / scale[:, None, None]
-                A[:, h, :h] = -1.0
-                A[:, :h, h] = -1.0
-                rhs = torch.zeros((R, h + 1, 1), dtype=torch.float64, device=self.dev)
-                rhs[:, h, 0] = -1.0
-                c = (torch.linalg.pinv(A) @ rhs)[:, :h, 0]                        # (R, h)
-                F = torch.einsum("rk,rkij->rij", c, torch.stack(b.hF, 1))
-            Fo = b.X.transpose(1, 2) @ F @ b.X + b.shift
-            _, C = torch.linalg.eigh(Fo)
-            C = (b.X @ C) * b.occ[:, None, :]
+            n = b.n
+            live = np.nonzero(~self.frozen[b.mol_np])[0]       # rows of molecules still iterating
+            if len(live) == 0:
+                continue
+            if len(live) == len(b.rows):
+                g, X, sh, occ = b.gidx2, b.X, b.shift, b.occ
+            else:
+                li = torch.tensor(live, device=self.dev)
+                g, X, sh, occ = b.gidx2[li], b.X[li], b.shift[li], b.occ[li]
+            R = len(live)
+            F = Ffull[g.reshape(-1)].view(R, n, n)
+            Fo = X.transpose(1, 2) @ F @ X + sh
+            _, C = syev_batched(Fo, stream=self.stream)     # one cuSOLVER call per bucket
+            C = (X @ C) * occ[:, None, :]
             Dn = C @ C.transpose(1, 2)
-            newP.index_copy_(0, b.sidx, Dn.reshape(-1)[b.svalid])
+            # padded positions target the trailing slot; their values are exact zeros
+            Pnew.index_copy_(0, g.reshape(-1), Dn.reshape(-1))
+        Pnew[2 * T_] = 0.0
         # restricted molecules: beta = alpha
-        rmask = torch.tensor(self.restricted, device=self.dev)[self.molid]
-        newP[T_:2 * T_] = torch.where(rmask, newP[:T_], newP[T_:2 * T_])
-        dPm = torch.zeros(nm, dtype=torch.float64, device=self.dev)
-        dPm.scatter_reduce_(0, self.molid, (newP[:T_] - self.P[:T_]).abs(), reduce="amax")
-        self.P.copy_(newP)
-        return E, emax, dPm
+        Pnew[T_:2 * T_] = torch.where(self.rmask, Pnew[:T_], Pnew[T_:2 * T_])
+        PA, PB = Pnew[:T_], Pnew[T_:2 * T_]
+        dens = (self.H + 0.5 * self.JT) * (PA + PB) + 0.5 * (self.K[:T_] * PA + self.K[T_:2 * T_] * PB)
+        E = torch.zeros(nm, dtype=torch.float64, device=self.dev).index_add_(0, self.molid, dens) + self.enn
+        out, avg = self.diis.step(Pnew[:2 * T_])
+        keep = self.frozen_t[self.molid2]
+        self.Pold.copy_(self.P)
+        self.P[:2 * T_] = torch.where(keep, self.P[:2 * T_], out)
+        return E, avg
 
-    def run(self, max_iter=60):
+    def run(self, max_iter=SCF_MAX):
         torch = self.torch
         t0 = time.perf_counter()
-        self._graph_ready = False
+        self._graph_ready = self.graph is not None
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        nm = len(self.mols)
+        T_ = self.total
         with torch.cuda.stream(self.stream):
+            ev0.record(self.stream)
+            self.frozen = np.zeros(nm, dtype=bool)
+            self.frozen_t = torch.zeros(nm, dtype=torch.bool, device=self.dev)
+            self.diis = DensityDIIS4(torch, self.P[:2 * T_], self.molid2, nm, self.nbf2)
             self._set_step(True)
+            self.t_build = self.t_tail = 0.0
+            eb0, eb1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            et1 = torch.cuda.Event(enable_timing=True)
             while self.iters < max_iter:
                 tb = time.perf_counter()
+                eb0.record(self.stream)
                 self._build()
+                eb1.record(self.stream)
                 if self.first:
                     self.first = False
                     self._set_step(False)     # later builds: density screen everywhere
                 elif not self._graph_ready:
                     self._graph_ready = True  # the next build is captured
-                E, emax, dPm = self._tail()
-                if self.iters == 0 and self.autotune:
+                E, avg = self._tail()
+                et1.record(self.stream)
+                if self.iters == 0 and self.autotune and not self._tuned:
                     # tile autotuner on the work of the difference-density builds that follow
-                    T_ = self.total
+                    self._tuned = True
                     torch.sub(self.P, self.Pold, out=self.dP)
                     self.batch.autotune(self.dP.data_ptr(), self.dP.data_ptr() + 8 * T_,
                                         stream=self.stream.cuda_stream)
-                h = torch.stack([E, emax, dPm]).cpu().numpy()
+                h = torch.stack([E, avg]).cpu().numpy()
                 self.build_seconds += time.perf_counter() - tb
-                E, emax, dPm = h
-                self.dE = E - self.energy
-                self.energy = E
-                self.emax, self.dPmax = emax, dPm
+                self.t_build += eb0.elapsed_time(eb1) / 1e3
+                self.t_tail += eb1.elapsed_time(et1) / 1e3
+                E, avg = h
+                live = ~self.frozen
+                prev = np.where(np.isnan(self.energy), 0.0, self.energy)
+                self.dE = np.where(live, E - prev, self.dE)
+                self.energy = np.where(live, E, self.energy)
+                self.avgdP = np.where(live, avg, self.avgdP)
                 self.iters += 1
-                conv = (np.abs(self.dE) < 0.01 * self.scf_conv) & (emax < 1e-6) & (dPm < 1e-6)
-                self.converged = conv
-                if conv.all():
+                self.iter_count = np.where(live, self.iters, self.iter_count)
+                conv = live & (np.abs(self.dE) <= self.scf_conv) & (avg <= self.scf_conv)
+                self.converged = self.converged | conv
+                self.frozen = self.frozen | conv
+                self.frozen_t.copy_(torch.tensor(self.frozen), non_blocking=False)
+                if self.frozen.all():
                     break
+            ev1.record(self.stream)
         self.stream.synchronize()
         self.seconds = time.perf_counter() - t0
+        self.device_seconds = ev0.elapsed_time(ev1) / 1e3
         return self.energy
 
     def close(self):

@@ -15,6 +15,7 @@
 // generated kernel launch per quartet class, and a finalize kernel that forms
 // JT = J + J^T, KA = -(K + K^T) (KB likewise, or KB = KA when restricted).
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
 #include <climits>
@@ -1785,5 +1786,66 @@ extern "C" int sqb200_batch_stats(sqb200_batch* b, long long* out, int n) {
   }
   long long v[6] = {q, pq, (long long)fl, shells, pairs, (long long)b->last_launches};
   for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
+  return SQB200_OK;
+}
+
+// ---------------------------------------------------------------- batched eigensolver
+//
+// The SCF tail's generalised eigenproblems, already reduced to standard form, for many
+// molecules of one padded size at once: cusolverDnXsyevBatched (one call per stack).
+
+namespace {
+struct SyevCtx {
+  cusolverDnHandle_t h = nullptr;
+  cusolverDnParams_t p = nullptr;
+  void* dwork = nullptr;
+  size_t dbytes = 0;
+  std::vector<char> hwork;
+  int* dinfo = nullptr;
+  long long ninfo = 0;
+};
+std::mutex g_syev_mu;
+std::map<int, SyevCtx> g_syev;
+}  // namespace
+
+extern "C" int sqb200_syev_batched(int device, int n, int batch, double* A, double* W, void* stream) {
+  if (n <= 0 || batch <= 0 || !A || !W) return fail(SQB200_EINVAL, "sqb200_syev_batched: bad argument");
+  std::lock_guard<std::mutex> lock(g_syev_mu);
+  CUDA_OK(cudaSetDevice(device));
+  SyevCtx& c = g_syev[device];
+  if (!c.h) {
+    if (cusolverDnCreate(&c.h) != CUSOLVER_STATUS_SUCCESS) return fail(SQB200_ECUDA, "cusolverDnCreate failed");
+    if (cusolverDnCreateParams(&c.p) != CUSOLVER_STATUS_SUCCESS) return fail(SQB200_ECUDA, "cusolverDnCreateParams failed");
+  }
+  if (cusolverDnSetStream(c.h, (cudaStream_t)stream) != CUSOLVER_STATUS_SUCCESS)
+    return fail(SQB200_ECUDA, "cusolverDnSetStream failed");
+  size_t db = 0, hb = 0;
+  if (cusolverDnXsyevBatched_bufferSize(c.h, c.p, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, A,
+                                        n, CUDA_R_64F, W, CUDA_R_64F, &db, &hb, batch) != CUSOLVER_STATUS_SUCCESS)
+    return fail(SQB200_ECUDA, "cusolverDnXsyevBatched_bufferSize failed");
+  if (db > c.dbytes || batch > c.ninfo) {
+    // the previous call's work may still run on another stream: wait before freeing
+    CUDA_OK(cudaDeviceSynchronize());
+    if (db > c.dbytes) {
+      cudaFree(c.dwork);
+      c.dwork = nullptr;
+      c.dbytes = 0;
+      CUDA_OK(cudaMalloc(&c.dwork, db));
+      c.dbytes = db;
+    }
+    if (batch > c.ninfo) {
+      cudaFree(c.dinfo);
+      c.dinfo = nullptr;
+      c.ninfo = 0;
+      CUDA_OK(cudaMalloc(&c.dinfo, sizeof(int) * (size_t)batch));
+      c.ninfo = batch;
+    }
+  }
+  if (hb > c.hwork.size()) c.hwork.resize(hb);
+  if (cusolverDnXsyevBatched(c.h, c.p, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, A, n,
+                             CUDA_R_64F, W, CUDA_R_64F, c.dwork, c.dbytes, hb ? c.hwork.data() : nullptr, hb,
+                             c.dinfo, batch) != CUSOLVER_STATUS_SUCCESS)
+    return fail(SQB200_ECUDA, "cusolverDnXsyevBatched failed");
+  CUDA_OK(cudaGetLastError());
   return SQB200_OK;
 }

@@ -26,6 +26,7 @@ EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_j
            "sqb200_peak_fma", "sqb200_batch_create", "sqb200_batch_destroy", "sqb200_batch_offsets",
            "sqb200_batch_set_step", "sqb200_batch_build_device", "sqb200_batch_stats",
            "sqb200_batch_autotune", "sqb200_jk_autotune", "sqb200_jk_tiles", "sqb200_jk_set_tiles",
+           "sqb200_syev_batched",
            "sqb200_last_error"]
 
 
@@ -69,6 +70,7 @@ def load_library(path=LIB_PATH):
     L.sqb200_jk_autotune.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                      ctypes.c_double, vp]
     L.sqb200_jk_tiles.argtypes = [vp, _i32p, ctypes.c_int]
+    L.sqb200_syev_batched.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
     L.sqb200_jk_set_tiles.argtypes = [vp, _i32p, ctypes.c_int]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
@@ -234,6 +236,19 @@ def peak_fma(device=0, iters=4096):
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(L.sqb200_peak_fma(device, iters, ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def syev_batched(A, stream=None):
+    """(eigenvalues, eigenvectors as columns) of a stack of symmetric FP64 CUDA matrices
+    (B, n, n), by one cusolverDnXsyevBatched call; A is not modified."""
+    import torch
+    L = load_library()
+    B_, n = A.shape[0], A.shape[-1]
+    V = A.contiguous().clone()
+    W = torch.empty((B_, n), dtype=torch.float64, device=A.device)
+    st = torch.cuda.current_stream(A.device) if stream is None else stream
+    _check(L.sqb200_syev_batched(A.device.index, n, B_, V.data_ptr(), W.data_ptr(), st.cuda_stream))
+    return W, V.transpose(1, 2)
 
 
 class JKBatch:

@@ -127,9 +127,25 @@ def xyz_text(atoms, comment="generated"):
     """XYZ file text (angstrom) in the layout readMolecule_XYZ expects (src/mol.c:92)."""
     lines = [str(len(atoms)), comment]
     for z, x, y, w in atoms:
-        lines.append("%-2s %20.12f %20.12f %20.12f" % (SYMBOLS[z], x, y, w))
+        lines.append("%-2s %20.12f %20.12f %20.12f" % (SYMBOLS[int(round(z))], x, y, w))
     return "\n".join(lines) + "\n"
 
 
 def n_electrons(atoms, charge=0):
     return sum(a[0] for a in atoms) - charge
+
+
+def organic_set(seed, count, heavy=(2, 20)):
+    """`count` seeded random closed-shell organics (random_organic) with a uniform number of
+    heavy atoms in [heavy[0], heavy[1]]: the batched-SCF workload."""
+    rng = np.random.default_rng(seed)
+    return [random_organic(rng, int(rng.integers(heavy[0], heavy[1] + 1))) for _ in range(count)]
+
+
+def remove_one_h(atoms, rng):
+    """The doublet radical of a closed-shell molecule: one hydrogen removed at random."""
+    hs = [i for i, a in enumerate(atoms) if a[0] == 1]
+    if not hs:
+        raise ValueError("no hydrogen to remove")
+    k = hs[int(rng.integers(len(hs)))]
+    return atoms[:k] + atoms[k + 1:]

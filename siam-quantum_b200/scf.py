@@ -2,11 +2,13 @@
 src/uhf.c:1171-1964, kept on the GPU).
 
 Per job all matrices (S, H, densities, J/K, Fock, DIIS history) live on the device in FP64 and
-every step runs on the job's own CUDA stream.  Each iteration builds J/K from the *difference*
-density with the reference's screening semantics (uhf.c:1594-1611 accumulates dJT/dKA/dKB the
-same way), forms F = H + JT + K, extrapolates with Pulay DIIS on the commutator FDS - SDF, and
-diagonalises in an orthonormal basis with a cuSOLVER FP64 eigensolver (torch.linalg.eigh).
-Conventions follow the reference: KA = -K[PA]; E = Enn + sum PT.H + 1/2 sum PT.JT
+every step runs on the job's own CUDA stream.  The loop is the reference's (src/uhf.c:1591-1783)
+with its defaults: J/K of the *difference* density accumulated into JT/KA/KB, F = H + JT + K,
+new densities from the lowest orbitals (a cuSOLVER FP64 eigensolve in an S-orthonormal basis in
+place of gen_sym_SomeEigen), the energy of those densities with the accumulated J/K, then the
+reference's 4-point density DIIS (conv_diis4, drag 0.25); converged when |dE| and the RMS
+density change are both <= SCFConv, at most 80 iterations.
+Conventions: KA = -K[PA]; E = Enn + sum PT.H + 1/2 sum PT.JT
 + 1/2 sum (PA.KA + PB.KB) (uhf_getEtotal, src/uhf.c:222-315); the integral cutoff is the 1STEP
 rule SCFConv / (nEA^2 + nEA nEB + nEB^2) / 50 evaluated on the identity-diagonal guess
 (src/uhf.c:1384-1399, 1465-1472); nEA/nEB from the multiplicity as get_nEA/get_nEB (src/mol.c).
@@ -46,6 +48,71 @@ def nuclear_repulsion(atoms_bohr):
     return e
 
 
+SCF_DRAG = 0.25     # reference default -SCFDRAG (src/option.c:526)
+SCF_MAX = 80        # reference default -SCFMAX (src/option.c:527)
+
+
+class DensityDIIS4:
+    """The reference's 4-point density DIIS, conv_diis4 (src/conv.c:606-844), applied to many
+    independent molecules at once.
+
+    Densities are flat vectors holding every molecule's alpha and beta blocks; `seg` gives the
+    molecule of each element, `nbf2` each molecule's nbf^2.  Per molecule, as the reference:
+    the residual of a step is d = P_new - P_in (P_in = the previous step's output); the first
+    three steps return the damped mix alpha P_new + (1 - alpha) P_in; later steps solve the
+    5 x 5 DIIS system on the last four residuals (B_xy = sum over both spins of d_x . d_y, rows
+    bordered by -1) and return sum_k c_k (P_in,k + d_k), falling back to the damped mix when the
+    newest residual grew (B33 > B22).  The RMS deviation sqrt(sum d^2 / nbf^2 / 2) is what
+    the reference tests against SCFConv."""
+
+    PAIRS = [(0, 0), (0, 1), (0, 2), (0, 3), (1, 1), (1, 2), (1, 3), (2, 2), (2, 3), (3, 3)]
+
+    def __init__(self, torch, P, seg, nseg, nbf2, alpha=SCF_DRAG):
+        self.torch = torch
+        self.seg, self.nseg, self.alpha = seg, nseg, alpha
+        self.nbf2 = nbf2.to(P.dtype)
+        self.Pin = [torch.zeros_like(P) for _ in range(3)] + [P.clone()]   # P0, P1, P2, P3
+        self.d = [torch.zeros_like(P) for _ in range(4)]                      # dP0 .. dP3
+        self.n = 1                                                            # nIter after the first call
+
+    def _segsum(self, x):
+        torch = self.torch
+        return torch.zeros(self.nseg, dtype=x.dtype, device=x.device).index_add_(0, self.seg, x)
+
+    def step(self, Pnew):
+        """(the next input density, RMS deviation per molecule)."""
+        torch = self.torch
+        P0, P1, P2, P3 = self.Pin
+        d3 = Pnew - P3
+        avg = torch.sqrt(self._segsum(d3 * d3) / self.nbf2 / 2.0)
+        d0, d1, d2 = self.d[0], self.d[1], self.d[2]
+        a = self.alpha
+        if self.n <= 3:
+            out = a * Pnew + (1.0 - a) * P3
+        else:
+            ds = [d0, d1, d2, d3]
+            Bv = {xy: self._segsum(ds[xy[0]] * ds[xy[1]]) for xy in self.PAIRS}
+            A = torch.zeros((self.nseg, 5, 5), dtype=Pnew.dtype, device=Pnew.device)
+            for (x, y), v in Bv.items():
+                A[:, x, y] = v
+                A[:, y, x] = v
+            A[:, 4, :4] = -1.0
+            A[:, :4, 4] = -1.0
+            rhs = torch.zeros((self.nseg, 5, 1), dtype=Pnew.dtype, device=Pnew.device)
+            rhs[:, 4, 0] = -1.0
+            c, info = torch.linalg.solve_ex(A, rhs)
+            c = c[:, :4, 0]
+            damp = (Bv[(3, 3)] > Bv[(2, 2)]) | (info != 0) | ~torch.isfinite(c).all(dim=1)
+            cd = torch.tensor([0.0, 0.0, 1.0 - a, a], dtype=Pnew.dtype, device=Pnew.device)
+            c = torch.where(damp[:, None], cd[None, :], c)
+            cs = c[self.seg]                                                  # per element
+            out = (cs[:, 3] * Pnew + cs[:, 2] * (P2 + d2) + cs[:, 1] * (P1 + d1) + cs[:, 0] * (P0 + d0))
+        self.d = [d1, d2, d3, None]          # d0 <- d1, d1 <- d2, d2 <- d3
+        self.Pin = [P1, P2, P3, out]
+        self.n += 1
+        return out, avg
+
+
 class SCFJob:
     """One molecule's SCF state, resident on one device.
 
@@ -54,7 +121,7 @@ class SCFJob:
     on `device` for the job's basis."""
 
     def __init__(self, atoms_angstrom, basis_name, charge=0, mult=None, restricted=None,
-                 scf_conv=1e-8, device=0, fp32_below=0.0, engine=None, diis_size=8):
+                 scf_conv=1e-8, device=0, fp32_below=0.0, engine=None):
         import torch
         self.torch = torch
         self.dev = device if isinstance(device, torch.device) else torch.device("cuda", device)
@@ -67,7 +134,6 @@ class SCFJob:
         if self.restricted and self.nea != self.neb:
             raise ValueError("restricted SCF needs a closed shell")
         self.scf_conv = scf_conv
-        self.diis_size = diis_size
         self.eng = engine if engine is not None else JKEngine(self.basis, device=self.dev.index)
         if fp32_below > 0:
             self.eng.set_precision(fp32_below)
@@ -95,9 +161,9 @@ class SCFJob:
             self.JT, self.KA, self.KB = z(), z(), z()
             self.dJT, self.dKA, self.dKB = z(), z(), z()
             self.PA_old, self.PB_old = z(), z()
-        self.diis_F, self.diis_E = [], []
+        self.diis = None
         self.energy, self.iters, self.converged, self.dE = None, 0, False, None
-        self.emax = self.dP = None
+        self.avgdP = None
         self.first = True
         self.seconds = 0.0
 
@@ -126,35 +192,13 @@ class SCFJob:
         C = self.X @ C[:, :nocc]
         return C @ C.T
 
-    def _diis(self, FA, FB, err):
-        torch = self.torch
-        self.diis_F.append((FA, FB))
-        self.diis_E.append(err)
-        if len(self.diis_F) > self.diis_size:
-            self.diis_F.pop(0)
-            self.diis_E.pop(0)
-        m = len(self.diis_F)
-        if m < 2:
-            return FA, FB
-        E = torch.stack([e.reshape(-1) for e in self.diis_E])
-        Bm = torch.zeros((m + 1, m + 1), dtype=torch.float64, device=self.dev)
-        Bm[:m, :m] = E @ E.T
-        # scale for conditioning: the solution's coefficients do not change
-        Bm[:m, :m] /= Bm[:m, :m].diagonal().max().clamp_min(1e-300)
-        Bm[m, :m] = -1.0
-        Bm[:m, m] = -1.0
-        rhs = torch.zeros((m + 1, 1), dtype=torch.float64, device=self.dev)
-        rhs[m, 0] = -1.0
-        c = (torch.linalg.pinv(Bm) @ rhs)[:m, 0]
-        FA = torch.einsum("k,kij->ij", c, torch.stack([f[0] for f in self.diis_F]))
-        FB = FA if self.restricted else torch.einsum("k,kij->ij", c, torch.stack([f[1] for f in self.diis_F]))
-        return FA, FB
-
     def update(self):
-        """After build_jk: accumulate J/K, energy, DIIS, new densities (on the job's stream).
-        Returns True when converged (|dE| < SCFConv/100, max |commutator| < 1e-6 and
-        max |dP| < 1e-6)."""
+        """After build_jk, one step of the reference's loop (src/uhf.c:1600-1730): accumulate
+        J/K, Fock, new densities from the lowest orbitals, the energy of those densities with
+        the accumulated J/K, then conv_diis4.  Returns True when |dE| <= SCFConv and the RMS
+        density deviation <= SCFConv (the reference's test)."""
         torch = self.torch
+        n = self.n
         with self._on_stream():
             self.JT += self.dJT
             self.KA += self.dKA
@@ -164,33 +208,27 @@ class SCFJob:
                 self.KB += self.dKB
             self.PA_old, self.PB_old = self.PA, self.PB
             FA = self.H + self.JT + self.KA
-            FB = FA if self.restricted else self.H + self.JT + self.KB
-            PT = self.PA + self.PB
-            e_t = ((PT * self.H).sum() + 0.5 * (PT * self.JT).sum()
-                   + 0.5 * ((self.PA * self.KA).sum() + (self.PB * self.KB).sum()))
-            errA = FA @ self.PA @ self.S
-            errA = errA - errA.T
-            if self.restricted:
-                err = errA
-            else:
-                errB = FB @ self.PB @ self.S
-                err = torch.cat([errA, errB - errB.T])
-            emax_t = err.abs().max()
-            FA, FB = self._diis(FA, FB, err)
-            self.PA = self._density(FA, self.nea)
-            self.PB = self.PA if self.restricted else self._density(FB, self.neb)
-            dP_t = (self.PA - self.PA_old).abs().max()
-            E, emax, dP = (float(v) for v in torch.stack([e_t, emax_t, dP_t]).cpu())
+            PA = self._density(FA, self.nea)
+            PB = PA if self.restricted else self._density(self.H + self.JT + self.KB, self.neb)
+            e_t = (((self.H + 0.5 * self.JT) * (PA + PB)).sum()
+                   + 0.5 * ((self.KA * PA).sum() + (self.KB * PB).sum()))
+            if self.diis is None:
+                self.diis = DensityDIIS4(torch, torch.cat([self.PA.reshape(-1), self.PB.reshape(-1)]),
+                                         torch.zeros(2 * n * n, dtype=torch.int64, device=self.dev), 1,
+                                         torch.tensor([n * n], device=self.dev))
+            out, avg = self.diis.step(torch.cat([PA.reshape(-1), PB.reshape(-1)]))
+            self.PA = out[:n * n].view(n, n)
+            self.PB = self.PA if self.restricted else out[n * n:].view(n, n)
+            E, avgdP = (float(v) for v in torch.stack([e_t, avg[0]]).cpu())
         E += self.enn
-        self.dE = None if self.energy is None else E - self.energy
+        self.dE = E - (0.0 if self.energy is None else self.energy)
         self.energy = E
         self.iters += 1
-        self.emax, self.dP = emax, dP
-        self.converged = (self.dE is not None and abs(self.dE) < 0.01 * self.scf_conv
-                          and emax < 1e-6 and dP < 1e-6)
+        self.avgdP = avgdP
+        self.converged = abs(self.dE) <= self.scf_conv and avgdP <= self.scf_conv
         return self.converged
 
-    def run(self, max_iter=100):
+    def run(self, max_iter=SCF_MAX):
         t0 = time.perf_counter()
         while self.iters < max_iter:
             self.build_jk()

@@ -5,13 +5,15 @@ seeded synthetic molecules and stores, per case, in <case>.npz:
   atoms (Z, x, y, z in angstrom), basis name,
   the reference's own genBasis arrays (nprim, lmn, xyz in bohr, exps, coefs, norms),
   the reference's basis-level Schwarz matrix (create_Schwarz),
-  the converged SCF energy and densities PA, PB (uhf(), -SCFACC=1STEP -SCFCONV=1e-8),
+  the converged SCF energy and densities PA, PB (uhf(), -SCFACC=1STEP -SCFCONV=1e-8) and the
+  number of SCF iterations uhf() took (scf_iters),
   the reference's one-electron matrices S, T, V (GTO_overlap, GTO_kinetic, GTO_nuclei),
   fresh reference J/K builds from the converged density at cutoff 1e-10:
     *_mem  : -MAXMEM=250 (first visit computes every Schwarz survivor, no density screen)
     *_dir  : -MAXMEM=0   (density screen on every quartet)
 Usage:  make -C oracle && python tests/golden/make_golden.py
         python tests/golden/make_golden.py --oneint   (add S, T, V to existing fixtures only)
+        python tests/golden/make_golden.py --iters    (add the reference's SCF iteration count)
 """
 import os
 import subprocess
@@ -94,6 +96,22 @@ def add_oneint():
         print(name, "S/T/V added, nbf", n)
 
 
+def add_scf_iters():
+    """Store the reference's SCF iteration count (1STEP, SCFConv 1e-8) in existing fixtures."""
+    for name, geom, bas, opts in CASES:
+        path = os.path.join(OUT, name + ".npz")
+        rec = dict(np.load(path, allow_pickle=True))
+        with tempfile.TemporaryDirectory() as d:
+            xyz = os.path.join(d, "m.xyz")
+            with open(xyz, "w") as f:
+                f.write(M.xyz_text(geom(), name))
+            res, _, _ = port.ref_scf(xyz, os.path.join(BASIS_DIR, bas + ".txt"),
+                                     ["-SCFACC=1STEP", "-SCFCONV=1e-8"] + list(opts))
+        rec["scf_iters"] = np.int64(res["iters"])
+        np.savez_compressed(path, **rec)
+        print(name, "reference SCF iterations", res["iters"])
+
+
 def main():
     for name, geom, bas, opts in CASES:
         atoms = geom()
@@ -110,7 +128,8 @@ def main():
             restricted = bool(np.array_equal(PA, PB))
             rec = dict(atoms=np.array(atoms), basis=bas, nprim=nprim, lmn=lmn, xyz=xyzs, exps=exps,
                        coefs=coefs, norms=norms, schwarz=S, energy=res["energy"], PA=PA, PB=PB,
-                       restricted=restricted, cutoff=1e-10, S=S1, T=T1, V=V1)
+                       restricted=restricted, cutoff=1e-10, S=S1, T=T1, V=V1,
+                       scf_iters=np.int64(res["iters"]))
             for tag, mm in (("mem", 250), ("dir", 0)):
                 JT, KA, KB, _ = port.ref_jk(xyz, bp, PA, None if restricted else PB,
                                             restricted=restricted, cutoff=1e-10, max_mem=mm)
@@ -120,4 +139,9 @@ def main():
 
 
 if __name__ == "__main__":
-    add_oneint() if "--oneint" in sys.argv[1:] else main()
+    if "--oneint" in sys.argv[1:]:
+        add_oneint()
+    elif "--iters" in sys.argv[1:]:
+        add_scf_iters()
+    else:
+        main()

@@ -49,8 +49,12 @@ def test_mixed_error_shrinks_with_tau(case):
     with open(os.path.join(ROOT, "gpurun_out", "mixed_jk_err_%s.json" % case), "w") as f:
         json.dump(dict(zip(map(str, TAUS), errs)), f)
     assert errs[0] < 1e-4
-    assert errs[-1] <= errs[0]
+    # monotone above FP64 rounding (1e-13 here); a molecule whose FP32 share is negligible at
+    # every tau sits at rounding level throughout
+    assert errs[-1] <= max(errs[0], 1e-13)
     assert errs[-1] < 1e-8
+    if case == "benzene_631gs":
+        assert errs[0] > 1e-12          # the FP32 forms did run
 
 
 @pytest.mark.gpu

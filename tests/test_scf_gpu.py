@@ -1,7 +1,8 @@
 """Device SCF tail: one-electron matrices from the GPU against the reference's own S, T, V
 (GTO_overlap/GTO_kinetic/GTO_nuclei, stored in the golden fixtures), and whole RHF/UHF SCF runs
-on the device (GPU J/K of difference densities, DIIS, cuSOLVER eigensolves) against the
-reference's converged energies (uhf(), -SCFACC=1STEP -SCFCONV=1e-8)."""
+on the device (GPU J/K of difference densities, the reference's density DIIS, cuSOLVER
+eigensolves) against the reference's converged energies and iteration counts (uhf(),
+-SCFACC=1STEP -SCFCONV=1e-8)."""
 import json
 import os
 
@@ -10,7 +11,7 @@ import pytest
 
 from conftest import GOLDEN_CASES, ROOT, golden, golden_basis, load_sqb200
 
-E_TOL = 1e-7     # Eh; the reference stops at |dE| < 1e-8, this driver at |dE| < 1e-10
+E_TOL = 1e-8     # Eh, total energy against the reference's uhf() (same loop, same test)
 
 
 def test_electron_counts_follow_multiplicity():
@@ -59,3 +60,4 @@ def test_device_scf_energy(case):
                    "seconds": secs}, f)
     assert job.converged
     assert err <= E_TOL, err
+    assert abs(iters - int(g["scf_iters"])) <= 1

@@ -1,7 +1,8 @@
 """Host logic of the device SCF driver (scf.SCFJob), on the CPU: the driver runs on torch CPU
 tensors with a stand-in J/K engine whose builds come from the oracle (the C restatement of the
 reference's J/K build) and whose one-electron matrices are the reference's own (golden S, T, V).
-Its converged energies must match the reference's uhf() energies.  The GPU runs of the same
+Its converged energies must match the reference's uhf() energies, in the same number of SCF
+iterations.  The GPU runs of the same
 driver with the CUDA engine are in test_scf_gpu.py."""
 import numpy as np
 import pytest
@@ -53,9 +54,11 @@ def test_scf_driver_reaches_reference_energy(case):
     eng = OracleJK(g)
     job = sqb.scf.SCFJob([tuple(a) for a in g["atoms"]], str(g["basis"]), device=torch.device("cpu"),
                          restricted=bool(g["restricted"]), engine=eng)
-    e = job.run(max_iter=60)
-    assert job.converged, (job.iters, job.dE, job.emax)
-    assert abs(e - float(g["energy"])) < 1e-7, e - float(g["energy"])
+    e = job.run()
+    assert job.converged, (job.iters, job.dE, job.avgdP)
+    # the reference's own loop (density DIIS, its convergence test): same energy, same steps
+    assert abs(e - float(g["energy"])) < 1e-9, e - float(g["energy"])
+    assert job.iters == int(g["scf_iters"])
     # first build: reference first visit (memory cutoff); later builds: full density screen
     assert eng.builds[0][1] == job.rmax_first and all(b[1] == float("inf") for b in eng.builds[1:])
     assert all(b[0] == job.cutoff for b in eng.builds)
