@@ -53,6 +53,11 @@ STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out ac
 # re-deriving the Boys function and R for more ket functions, at more registers); which form a
 # class runs is chosen by measurement (sqb200_jk_autotune)
 STATE_MAX_WIDE = int(os.environ.get("SQB_STATE_MAX_WIDE", "128"))
+# the wide form keeps its contracted-block accumulators in shared memory instead (one slot per
+# thread, thread-fastest): only the Hermite intermediates G (at most G_MAX doubles) stay in
+# registers, so a pass can hold more ket functions without spilling
+WIDE_SMEM = int(os.environ.get("SQB_WIDE_SMEM", "0"))
+G_MAX = int(os.environ.get("SQB_G_MAX", "48"))
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
 F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
 MIN_BLOCKS = int(os.environ.get("SQB_MINB", "0"))   # __launch_bounds__ min CTAs per SM (0 = none)
@@ -163,15 +168,21 @@ def alg_prim_flops(fk, Hb, rt, fma):
     return 9 + 2 + 3 + 5 + boys_flops(L) + 2 + L + (L + 1) + rf + 2 * ncons
 
 
-def n_passes(bra, ket, state_max):
+def ket_per_pass(bra, ket, state_max, smem_o=False):
     fb, _, _ = etable(bra)
     fk, _, _ = etable(ket)
     Hb = {h for f in fb for h in nz(f)}
-    per = max(1, state_max // (len(Hb) + len(fb)))
+    per = max(1, (G_MAX // len(Hb)) if smem_o else state_max // (len(Hb) + len(fb)))
+    return min(per, len(fk))
+
+
+def n_passes(bra, ket, state_max, smem_o=False):
+    fk, _, _ = etable(ket)
+    per = ket_per_pass(bra, ket, state_max, smem_o)
     return (len(fk) + per - 1) // per
 
 
-def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
+def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False):
     """Return (kernel source, metadata) for class (bra|ket) and spin 'R' or 'U'.  prec "F"
     emits the mixed form: primitive setup, prefactor cut and Boys function in FP64, Hermite
     integrals, E tables and contracted accumulators in FP32, digestion into the FP64 J/K
@@ -190,11 +201,12 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
     nc, nd = len(COMP[ket[0]]), len(COMP[ket[1]])
     NB = 5 + len(layb)
     NK = 5 + len(layk)
-    per = max(1, (STATE_MAX if state_max is None else state_max) // (len(Hb) + nab))
+    per = ket_per_pass(bra, ket, STATE_MAX if state_max is None else state_max, smem_o)
     blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
     name = "jk_%s_%s_%s%s%s" % (bra, ket, spin, "_f32" if F32 else "", suffix)
+    SO = smem_o and not F32
     fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks),
-          "alg_prim": alg_prim_flops(fk, Hb, RT, FMA)}
+          "alg_prim": alg_prim_flops(fk, Hb, RT, FMA), "o_dbl": nab * per if SO else 0}
 
     em = Emitter()
     out = []
@@ -206,6 +218,8 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
         em("float* __restrict__ sbra = sbra_f32;")
     else:
         em("extern __shared__ double sbra[];")
+    if SO:
+        em("double* __restrict__ so = sbra + a.so_off;    // contracted-block accumulators, thread-fastest")
     em("const sqb::WorkItem it = items[blockIdx.x];")
     em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
     em("const sqb::MolRec mr = a.mols[it.mol];        // the molecule of this work item")
@@ -252,9 +266,12 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
     for bi, blk in enumerate(blocks):
         em("case %d: {  // ket functions %s" % (bi, blk))
         em.ind += 1
-        for ab in range(nab):
-            for cd in blk:
-                em("%s o%d_%d = 0;" % (RT, ab, cd))
+        if SO:
+            em("for (int x = 0; x < %d; ++x) so[x * %d + threadIdx.x] = 0.0;" % (nab * per, CTA))
+        else:
+            for ab in range(nab):
+                for cd in blk:
+                    em("%s o%d_%d = 0;" % (RT, ab, cd))
         em("for (int i = grp; i < nbp; i += isplit) {")
         em.ind += 1
         em("const %s* __restrict__ bi = sbra + i * %d;" % (RT, NB))
@@ -272,7 +289,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
             # computed, and its Boys-table row is fetched at the end of iteration j
             em("double nq = 0.0, nQx = 0.0, nQy = 0.0, nQz = 0.0, nkq = 0.0;")
             for (cd, k, e, sg) in kent:
-                em("double nek%d_%d = 0.0;" % (cd, k))
+                em("%s nek%d_%d = 0;" % (RT, cd, k))
             em("if (nkp > 0) { nq = kprim[0]; nQx = kprim[1]; nQy = kprim[2]; nQz = kprim[3]; nkq = kprim[4];")
             for (cd, k, e, sg) in kent:
                 em("  nek%d_%d = %skprim[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
@@ -282,8 +299,8 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
         if PREFETCH:
             em("const double q = nq, Qx = nQx, Qy = nQy, Qz = nQz, kq = nkq;")
             for (cd, k, e, sg) in kent:
-                em("const double ek%d_%d = nek%d_%d;" % (cd, k, cd, k))
-            em("if (j + 1 < nkp) { const double* __restrict__ kn = kprim + (j + 1) * %d;" % NK)
+                em("const %s ek%d_%d = nek%d_%d;" % (RT, cd, k, cd, k))
+            em("if (j + 1 < nkp) { const %s* __restrict__ kn = kprim + (j + 1) * %d;" % (RT, NK))
             em("  nq = kn[0]; nQx = kn[1]; nQy = kn[2]; nQz = kn[3]; nkq = kn[4];")
             for (cd, k, e, sg) in kent:
                 em("  nek%d_%d = %skn[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
@@ -342,6 +359,20 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
         # flush: o[ab][cd] += sum_h Eb[ab][h] g[cd][h]
         ff = 0
         for ab in range(nab):
+            if SO:
+                hs = list(enumerate(nz(fb[ab])))
+                em("{")
+                for k, h in hs:
+                    em("  const double eb%d = bi[%d];" % (k, 5 + offb[ab] + k))
+                for ci, cd in enumerate(blk):
+                    slot = "so[%d * %d + threadIdx.x]" % (ab * per + ci, CTA)
+                    em("  { double t = %s;" % slot)
+                    for k, h in hs:
+                        em("    t = fma(eb%d, g%d_%d, t);" % (k, cd, hidx[h]))
+                        ff += 2
+                    em("    %s = t; }" % slot)
+                em("}")
+                continue
             for k, h in enumerate(nz(fb[ab])):
                 e = offb[ab] + k
                 em("{ const %s eb = bi[%d];" % (RT, 5 + e))
@@ -354,6 +385,10 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix=""):
         fl["prim"] += pf
         fl["flush"] += ff
         # digestion of this block
+        if SO:
+            for ab in range(nab):
+                for ci, cd in enumerate(blk):
+                    em("const double o%d_%d = so[%d * %d + threadIdx.x];" % (ab, cd, ab * per + ci, CTA))
         qf = emit_digest(em, spin, blk, nab, na, nb_, nd)
         fl["quartet"] += qf
         em.ind -= 1
@@ -692,7 +727,13 @@ def main():
                 src.append(s2)
                 m["ws"] = m2
             m["wide"] = None
-            if n_passes(bra, ket, STATE_MAX_WIDE) < n_passes(bra, ket, STATE_MAX):
+            if WIDE_SMEM:
+                fb_, _, _ = etable(bra)
+                if len(fb_) * ket_per_pass(bra, ket, 0, True) >= 8:
+                    s4, m4 = gen_class(bra, ket, spin, "D", None, "_w", smem_o=True)
+                    src.append(s4)
+                    m["wide"] = m4
+            elif n_passes(bra, ket, STATE_MAX_WIDE) < n_passes(bra, ket, STATE_MAX):
                 s4, m4 = gen_class(bra, ket, spin, "D", STATE_MAX_WIDE, "_w")
                 src.append(s4)
                 m["wide"] = m4
@@ -743,11 +784,11 @@ def main():
         reg.append('   %d,' % r["flops"]["alg_prim"])
         wr, wu = r["wide"], u["wide"]
         if wr:
-            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d, %d},' % (
                 wr["flops"]["passes"], wr["name"], wu["name"], wr["flops"]["prim"], wr["flops"]["flush"],
-                wr["flops"]["quartet"]))
+                wr["flops"]["quartet"], wr["flops"]["o_dbl"]))
         else:
-            reg.append('   0, nullptr, nullptr, 0, 0, 0},')
+            reg.append('   0, nullptr, nullptr, 0, 0, 0, 0},')
     reg.append("};")
     reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
     reg.append("}  // namespace sqb")

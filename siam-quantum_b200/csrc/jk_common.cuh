@@ -69,7 +69,8 @@ struct JKArgs {
                                // [2] bra-primitive flushes, [3] digestions
   const MolRec* mols;          // per-molecule offsets, sizes and cutoffs (WorkItem::mol)
   int same_class;              // bra and ket pairs come from one class (pair identity possible)
-  int pad;
+  int so_off;                  // doubles from the start of dynamic shared memory to the
+                               // accumulator slots of the shared-memory wide form
   const float* bra_prims_f;    // FP32 copies of the primitive records (mixed-precision kernels)
   const float* ket_prims_f;
 };

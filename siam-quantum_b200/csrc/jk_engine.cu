@@ -745,11 +745,21 @@ struct SegLaunch {
 
 // The form of class kernel v (v >= K: FP32 form) for spin uhf; wide selects the wide-tile FP64
 // form where the class has one.
-void pick_form(const sqb::ClassKernel& K, bool f32, int uhf, bool wide, const void** fn, int* passes) {
-  if (f32) { *fn = uhf ? K.fn_u32 : K.fn_r32; *passes = K.passes32; return; }
-  if (wide && K.fn_rw) { *fn = uhf ? K.fn_uw : K.fn_rw; *passes = K.passes_w; return; }
+// Returns true when the wide form was picked.
+bool pick_form(const sqb::ClassKernel& K, bool f32, int uhf, bool wide, const void** fn, int* passes) {
+  if (f32) { *fn = uhf ? K.fn_u32 : K.fn_r32; *passes = K.passes32; return false; }
+  if (wide && K.fn_rw) { *fn = uhf ? K.fn_uw : K.fn_rw; *passes = K.passes_w; return true; }
   *fn = uhf ? K.fn_u : K.fn_r;
   *passes = K.passes;
+  return false;
+}
+
+// Shared-memory accumulators of the wide form: the region follows the staged bra primitives.
+void add_acc_region(const sqb::ClassKernel& K, bool wide_used, SegLaunch& L) {
+  if (!wide_used || K.w_o_dbl <= 0) return;
+  const size_t off = (L.smem + 15) / 16 * 16;
+  L.a.so_off = (int)(off / sizeof(double));
+  L.smem = off + (size_t)K.w_o_dbl * L.block.x * sizeof(double);
 }
 
 // Raise a kernel's dynamic shared-memory limit once per (device, kernel, size class), so that a
@@ -808,7 +818,9 @@ SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const dou
   if (ws) {
     L.fn = uhf ? K.ws_u : K.ws_r;
   } else {
-    pick_form(K, f32, uhf, wide < 0 ? (c->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
+    const bool wu = pick_form(K, f32, uhf, wide < 0 ? (c->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
+    L.block = dim3(128);
+    add_acc_region(K, wu, L);
   }
   L.grid = dim3(w->count[s], passes);
   L.block = dim3(ws ? 32 * K.ws_warps : 128);
@@ -1677,9 +1689,10 @@ SegLaunch seg_batch(sqb200_batch* b, size_t s, const double* dPA, const double* 
   L.items = b->d_items + b->first[s];
   L.smem = (size_t)B.max_nprim * B.stride * (f32 ? sizeof(float) : sizeof(double));
   int passes = 1;
-  pick_form(K, f32, uhf, wide < 0 ? (b->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
+  const bool wu = pick_form(K, f32, uhf, wide < 0 ? (b->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
   L.grid = dim3(b->count[s], passes);
   L.block = dim3(128);
+  add_acc_region(K, wu, L);
   return L;
 }
 

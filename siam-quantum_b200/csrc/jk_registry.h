@@ -39,6 +39,7 @@ struct ClassKernel {
   const void* fn_rw;
   const void* fn_uw;
   int w_flops_prim, w_flops_flush, w_flops_quartet;
+  int w_o_dbl;            // doubles per thread of the wide form's shared-memory accumulators (0: registers)
 };
 
 extern const ClassKernel kClassKernels[];

@@ -200,7 +200,8 @@ class JKEngine:
         _check(_lib.sqb200_jk_profile_read(self._ctx, rows, 200, ctypes.byref(n)))
         out = []
         for r in rows[: 6 * n.value].reshape(-1, 6):
-            out.append({"class": _lib.sqb200_jk_class_name(int(r[0])).decode(), "launches": int(r[1]),
+            out.append({"class": _lib.sqb200_jk_class_name(int(r[0])).decode(), "index": int(r[0]),
+                        "launches": int(r[1]),
                         "ms": float(r[2]), "flops": float(r[3]), "prim_quartets": int(r[4]),
                         "quartets": int(r[5])})
         return out
