@@ -175,8 +175,9 @@ int sqb200_batch_stats(sqb200_batch *batch, long long *out, int n);
  * matrices stored back to back in A (device memory), in one cusolverDnXsyevBatched call on
  * `stream`.  On return eigenvector k of matrix b is row k of A's b-th block (A read row-major).
  * The SCF tail's eigensolve for many molecules of one padded size (in place of the
- * reference's gen_sym_SomeEigen, src/lin.c:195, per molecule).  Asynchronous; grows a
- * per-device workspace when needed (synchronising the device then). */
+ * reference's gen_sym_SomeEigen, src/lin.c:195, per molecule).  Asynchronous; keeps one
+ * cuSOLVER handle and workspace per (device, stream), grown when needed (synchronising that
+ * stream then), so calls on different streams may overlap. */
 int sqb200_syev_batched(int device, int n, int batch, double *A, double *W, void *stream);
 
 /* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,

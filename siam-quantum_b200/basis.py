@@ -85,6 +85,7 @@ def build_basis(atoms_bohr, name):
     tab = basis_table(name)
     nprim, lmn, center, exps, coefs, norms = [], [], [], [], [], []
     for z, x, y, w in atoms_bohr:
+        z = int(round(z))
         recs = tab.get(str(z))
         if recs is None:
             raise ValueError("element Z=%d not in basis %s" % (z, name))

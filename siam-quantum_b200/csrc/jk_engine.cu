@@ -1817,15 +1817,17 @@ struct SyevCtx {
   int* dinfo = nullptr;
   long long ninfo = 0;
 };
+// one handle and workspace per (device, stream): calls on different streams may run on the
+// GPU at the same time and must not share a workspace
 std::mutex g_syev_mu;
-std::map<int, SyevCtx> g_syev;
+std::map<std::pair<int, void*>, SyevCtx> g_syev;
 }  // namespace
 
 extern "C" int sqb200_syev_batched(int device, int n, int batch, double* A, double* W, void* stream) {
   if (n <= 0 || batch <= 0 || !A || !W) return fail(SQB200_EINVAL, "sqb200_syev_batched: bad argument");
   std::lock_guard<std::mutex> lock(g_syev_mu);
   CUDA_OK(cudaSetDevice(device));
-  SyevCtx& c = g_syev[device];
+  SyevCtx& c = g_syev[{device, stream}];
   if (!c.h) {
     if (cusolverDnCreate(&c.h) != CUSOLVER_STATUS_SUCCESS) return fail(SQB200_ECUDA, "cusolverDnCreate failed");
     if (cusolverDnCreateParams(&c.p) != CUSOLVER_STATUS_SUCCESS) return fail(SQB200_ECUDA, "cusolverDnCreateParams failed");
@@ -1837,8 +1839,8 @@ extern "C" int sqb200_syev_batched(int device, int n, int batch, double* A, doub
                                         n, CUDA_R_64F, W, CUDA_R_64F, &db, &hb, batch) != CUSOLVER_STATUS_SUCCESS)
     return fail(SQB200_ECUDA, "cusolverDnXsyevBatched_bufferSize failed");
   if (db > c.dbytes || batch > c.ninfo) {
-    // the previous call's work may still run on another stream: wait before freeing
-    CUDA_OK(cudaDeviceSynchronize());
+    // the previous call on this stream may still run: wait before freeing its workspace
+    CUDA_OK(cudaStreamSynchronize((cudaStream_t)stream));
     if (db > c.dbytes) {
       cudaFree(c.dwork);
       c.dwork = nullptr;

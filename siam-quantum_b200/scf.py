@@ -23,7 +23,7 @@ import numpy as np
 
 from . import basis as B
 from . import molecules as M
-from .engine import JKEngine
+from .engine import JKEngine, syev_batched
 
 
 def electrons(atoms, charge=0, mult=None):
@@ -188,15 +188,20 @@ class SCFJob:
 
     def _density(self, F, nocc):
         Fo = self.X.T @ F @ self.X
-        _, C = self.torch.linalg.eigh(Fo)
+        if self.dev.type == "cuda":
+            # cuSOLVER without a host synchronisation (torch.linalg.eigh checks its status on
+            # the host), so that several jobs' steps can be in flight at once
+            _, C = syev_batched(Fo.unsqueeze(0), stream=self.stream)
+            C = C[0]
+        else:
+            _, C = self.torch.linalg.eigh(Fo)
         C = self.X @ C[:, :nocc]
         return C @ C.T
 
-    def update(self):
-        """After build_jk, one step of the reference's loop (src/uhf.c:1600-1730): accumulate
-        J/K, Fock, new densities from the lowest orbitals, the energy of those densities with
-        the accumulated J/K, then conv_diis4.  Returns True when |dE| <= SCFConv and the RMS
-        density deviation <= SCFConv (the reference's test)."""
+    def update_launch(self):
+        """Enqueue, after build_jk, one step of the reference's loop (src/uhf.c:1600-1730):
+        accumulate J/K, Fock, new densities from the lowest orbitals, the energy of those
+        densities with the accumulated J/K, then conv_diis4.  Nothing is read back."""
         torch = self.torch
         n = self.n
         with self._on_stream():
@@ -219,7 +224,13 @@ class SCFJob:
             out, avg = self.diis.step(torch.cat([PA.reshape(-1), PB.reshape(-1)]))
             self.PA = out[:n * n].view(n, n)
             self.PB = self.PA if self.restricted else out[n * n:].view(n, n)
-            E, avgdP = (float(v) for v in torch.stack([e_t, avg[0]]).cpu())
+            self._pending = torch.stack([e_t, avg[0]])
+
+    def update_finish(self):
+        """Read the step's energy and RMS density change (synchronises the job's stream) and
+        apply the reference's test: True when |dE| <= SCFConv and RMS dP <= SCFConv."""
+        with self._on_stream():
+            E, avgdP = (float(v) for v in self._pending.cpu())
         E += self.enn
         self.dE = E - (0.0 if self.energy is None else self.energy)
         self.energy = E
@@ -227,6 +238,11 @@ class SCFJob:
         self.avgdP = avgdP
         self.converged = abs(self.dE) <= self.scf_conv and avgdP <= self.scf_conv
         return self.converged
+
+    def update(self):
+        """update_launch + update_finish."""
+        self.update_launch()
+        return self.update_finish()
 
     def run(self, max_iter=SCF_MAX):
         t0 = time.perf_counter()
