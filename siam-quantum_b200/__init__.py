@@ -8,9 +8,10 @@ Python package is the host-side binding used by tests and the benchmark:
   scf        device-resident RHF/UHF SCF around the GPU Fock build (SCFJob)
   batch_scf  many molecules' SCF together: batched Fock builds in a CUDA graph (BatchSCF)
   serve      served stream of SCF jobs with continuous batching and HBM admission (Server)
+  checkpoint the reference's checkpoint files: read, write, and the projected orbital guess
 
 The directory name is not a Python identifier; import it with `load_package()` from a
 checkout root or via importlib (see tests/conftest.py).
 """
-from . import basis, batch_scf, engine, molecules, scf, serve  # noqa: F401
+from . import basis, batch_scf, checkpoint, engine, molecules, scf, serve  # noqa: F401
 from .engine import JKBatch, JKEngine, SQB200Error, load_library  # noqa: F401

@@ -121,7 +121,10 @@ class SCFJob:
     on `device` for the job's basis."""
 
     def __init__(self, atoms_angstrom, basis_name, charge=0, mult=None, restricted=None,
-                 scf_conv=1e-8, device=0, fp32_below=0.0, engine=None):
+                 scf_conv=1e-8, device=0, fp32_below=0.0, engine=None, guess=None):
+        """`guess`: None for the reference's identity-diagonal guess, or a checkpoint (a path or
+        the dict of checkpoint.read_checkpoint) whose orbitals are projected onto this basis as
+        the reference's -GUESS=CHECK does."""
         import torch
         self.torch = torch
         self.dev = device if isinstance(device, torch.device) else torch.device("cuda", device)
@@ -130,6 +133,7 @@ class SCFJob:
         self.atoms = M.to_bohr(atoms_angstrom)
         self.basis = B.build_basis(self.atoms, basis_name)
         self.nea, self.neb, self.mult = electrons(atoms_angstrom, charge, mult)
+        self.charge = charge
         self.restricted = (self.mult == 1) if restricted is None else bool(restricted)
         if self.restricted and self.nea != self.neb:
             raise ValueError("restricted SCF needs a closed shell")
@@ -144,7 +148,19 @@ class SCFJob:
         XYZ = np.array([a[1:] for a in self.atoms], dtype=np.float64)
         S, T, V = self.eng.oneint(Z, XYZ)
         self.enn = nuclear_repulsion(self.atoms)
-        sa, sb = self.nea, self.neb                  # sums of the identity-diagonal guess
+        PAg = PBg = None
+        if guess is not None:
+            from . import checkpoint as CK
+            chk = CK.read_checkpoint(guess) if isinstance(guess, str) else guess
+            if [int(a[0]) for a in chk["atoms"]] != [int(a[0]) for a in self.atoms]:
+                raise ValueError("checkpoint holds a different molecule")
+            CA, CB = CK.project_orbitals(chk, self.basis, S)
+            PAg = CA[:self.nea].T @ CA[:self.nea]
+            PBg = CB[:self.neb].T @ CB[:self.neb]
+            sa, sb = float(PAg.sum()), float(PBg.sum())
+        else:
+            sa, sb = self.nea, self.neb              # sums of the identity-diagonal guess
+        # the reference's cutoff rule on the sums of all guess-density elements (src/uhf.c:1465-1472)
         self.cutoff = scf_conv / (sa * sa + sa * sb + sb * sb) / 50.0
         self.rmax_first = self.eng.mem_cutoff(self.cutoff, 250)
         with self._on_stream():
@@ -153,10 +169,14 @@ class SCFJob:
             self.H = torch.tensor(T + V, **f64)
             w, U = torch.linalg.eigh(self.S)
             self.X = U * w.rsqrt()                   # canonical orthogonaliser: X^T S X = 1
-            tr = float(torch.trace(self.S))
-            eye = torch.eye(n, **f64)
-            self.PA = eye * (self.nea / tr)
-            self.PB = eye * (self.neb / tr)
+            if PAg is not None:
+                self.PA = torch.tensor(PAg, **f64)
+                self.PB = torch.tensor(PBg, **f64)
+            else:
+                tr = float(torch.trace(self.S))
+                eye = torch.eye(n, **f64)
+                self.PA = eye * (self.nea / tr)
+                self.PB = eye * (self.neb / tr)
             z = lambda: torch.zeros((n, n), **f64)
             self.JT, self.KA, self.KB = z(), z(), z()
             self.dJT, self.dKA, self.dKB = z(), z(), z()
@@ -213,8 +233,10 @@ class SCFJob:
                 self.KB += self.dKB
             self.PA_old, self.PB_old = self.PA, self.PB
             FA = self.H + self.JT + self.KA
+            self.FA = FA
+            self.FB = FA if self.restricted else self.H + self.JT + self.KB
             PA = self._density(FA, self.nea)
-            PB = PA if self.restricted else self._density(self.H + self.JT + self.KB, self.neb)
+            PB = PA if self.restricted else self._density(self.FB, self.neb)
             e_t = (((self.H + 0.5 * self.JT) * (PA + PB)).sum()
                    + 0.5 * ((self.KA * PA).sum() + (self.KB * PB).sum()))
             if self.diis is None:
@@ -254,6 +276,26 @@ class SCFJob:
             self.stream.synchronize()
         self.seconds = time.perf_counter() - t0
         return self.energy
+
+    def orbitals(self):
+        """All orbitals and orbital energies of the last Fock matrices, as the reference saves
+        them after its loop (gen_sym_eigen + normalizeC, src/uhf.c:1840-1843): (CA, CB, eA, eB)
+        as numpy arrays, orbital i in row i."""
+        out = []
+        for F in (self.FA, self.FB):
+            with self._on_stream():
+                w, C = self.torch.linalg.eigh(self.X.T @ F @ self.X)
+                C = (self.X @ C).T
+            out.append((C.cpu().numpy(), w.cpu().numpy()))
+        return out[0][0], out[1][0], out[0][1], out[1][1]
+
+    def save_checkpoint(self, path):
+        """Write the reference's checkpoint file (-SCHECK) for this job."""
+        from . import checkpoint as CK
+        CA, CB, eA, eB = self.orbitals()
+        CK.write_checkpoint(path, self.atoms, self.charge, self.mult, self.basis, self.energy,
+                            self.dE if self.dE is not None else 0.0,
+                            self.avgdP if self.avgdP is not None else 0.0, CA, CB, eA, eB)
 
     def close(self):
         self.eng.close()
