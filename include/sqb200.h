@@ -180,6 +180,26 @@ int sqb200_batch_stats(sqb200_batch *batch, long long *out, int n);
  * stream then), so calls on different streams may overlap. */
 int sqb200_syev_batched(int device, int n, int batch, double *A, double *W, void *stream);
 
+/* Gradient of the SCF energy with respect to the natom nuclear positions (bohr), written to
+ * grad (natom x 3, hartree/bohr; the reference prints forces = -grad): nuclear repulsion,
+ * -sum W dS, sum PT d(T + V) with the Hellmann-Feynman terms, and the two-electron term of
+ * GradEri_ShellSet_Parallel (src/grad.c:1734) -- as uhf_force (src/grad.c:2155) assembles
+ * them.  PA, PB: the densities of the final orbitals; W: the energy-weighted density
+ * sum_i e_i C_i C_i^T over the occupied orbitals of both spins (host arrays, nbf*nbf).  Every
+ * basis function must sit on one of the nuclei.  Synchronous. */
+int sqb200_gradient(sqb200_jk *ctx, int natom, const double *Z, const double *axyz,
+                    const double *PA, const double *PB, const double *W, double *grad);
+
+/* One or more terms of sqb200_gradient (bitwise or of SQB200_GRAD_*): nuclear repulsion,
+ * sum PT d(T + V) with the Hellmann-Feynman terms, -sum W dS, the two-electron term. */
+#define SQB200_GRAD_NUCLEAR 1
+#define SQB200_GRAD_HCORE   2
+#define SQB200_GRAD_OVERLAP 4
+#define SQB200_GRAD_ERI     8
+#define SQB200_GRAD_ALL     15
+int sqb200_gradient_terms(sqb200_jk *ctx, int natom, const double *Z, const double *axyz,
+                          const double *PA, const double *PB, const double *W, int terms, double *grad);
+
 /* Basis-level Schwarz matrix sqrt|(pq|pq)| on the device (create_Schwarz,
  * src/matrix.c:389-440), written to the host array S (nbf*nbf). */
 int sqb200_jk_schwarz(sqb200_jk *ctx, double *S);

@@ -158,3 +158,12 @@ def ref_oneint(xyz_path, basis_path, n):
         ref_run(["oneint", xyz_path, basis_path, out])
         m = np.fromfile(out, dtype=np.float64).reshape(3, n, n)
         return m[0], m[1], m[2]
+
+
+def ref_force(xyz_path, basis_path, options=()):
+    """Forces (natom, 3) of the reference's uhf_force after uhf(), and the energy."""
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "f.bin")
+        res = ref_run(["force", xyz_path, basis_path, out] + list(options))
+        F = np.fromfile(out, dtype=np.float64).reshape(3, -1).T
+    return F, res

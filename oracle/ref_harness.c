@@ -17,6 +17,9 @@
  *   sqref scf     <xyz> <basis> <densout|-> [reference options...]
  *                 uhf() (src/uhf.c:1171) as sq.c:152-415 drives it; prints the total energy
  *                 with 12 decimals on stderr and writes PA,PB of the final orbitals
+ *   sqref force   <xyz> <basis> <out> [reference options...]
+ *                 uhf() then uhf_force() (src/grad.c:2155): writes the forces Fx, Fy, Fz
+ *                 (3*nAtom doubles, hartree/bohr; force = -gradient) and prints the energy
  *   sqref oneint  <xyz> <basis> <out>
  *                 S, T, V as uhf() builds them (src/uhf.c:1307-1334: GTO_overlap,
  *                 GTO_kinetic, GTO_nuclei); writes S,T,V (3*n*n doubles)
@@ -32,6 +35,7 @@
 #include "matrix.h"
 #include "option.h"
 #include "uhf.h"
+#include "grad.h"
 
 static double now_s(void){
 	struct timespec t; clock_gettime(CLOCK_MONOTONIC, &t);
@@ -170,6 +174,35 @@ int main(int argc, char **argv){
 			double *out[2] = {PA, PB};
 			write_mats(argv[4], n, 2, out);
 		}
+		return 0;
+	}
+
+	if(!strcmp(cmd, "force") && argc >= 5){
+		int na = argc - 2;
+		char **pa = calloc(na + 1, sizeof(char *));
+		pa[0] = "sq"; pa[1] = argv[2]; pa[2] = argv[3];
+		for(int i = 5; i < argc; i++) pa[i - 2] = argv[i];
+		struct option_t opt;
+		parse_option(&opt, na, pa);
+		opt.nCPU = 1;
+		struct Molecule_t *mol;
+		struct GTOBasis_t *g = load_basis(argv[2], argv[3], &n, &mol);
+		mol->Q = opt.molCharge;
+		if(opt.multiplicity == 0) opt.multiplicity = (get_nElectron(mol) % 2 == 0) ? 1 : 2;
+		if(opt.multiplicity > 1) opt.restricted = 0;
+		int nEA = get_nEA(mol, opt.multiplicity), nEB = get_nEB(mol, opt.multiplicity);
+		double *CA = calloc((size_t)n * n, 8), *CB = calloc((size_t)n * n, 8);
+		double *eA = calloc(n, 8), *eB = calloc(n, 8);
+		double E = uhf(n, g, mol, nEA, nEB, CA, CB, eA, eB, &opt);
+		double *F = calloc(3 * (size_t)mol->nAtom, 8);
+		uhf_force(n, g, mol, nEA, nEB, CA, CB, eA, eB, &opt, F, F + mol->nAtom, F + 2 * mol->nAtom);
+		fflush(stdout);
+		fprintf(stderr, "RESULT energy=%.12f nbf=%d natom=%d\n", E, n, mol->nAtom);
+		double *out[1] = {F};
+		FILE *f = fopen(argv[4], "wb");
+		if(!f){ fprintf(stderr, "cannot write %s\n", argv[4]); exit(2); }
+		fwrite(out[0], sizeof(double), 3 * (size_t)mol->nAtom, f);
+		fclose(f);
 		return 0;
 	}
 

@@ -388,11 +388,12 @@ __device__ void oe_hermite(double p, double xpa, double xpb, int la, int lb, dou
         double v;
         if (i == 0 && j == 0) v = (t == 0) ? 1.0 : 0.0;
         else if (i > 0) {
-          v = xpa * E[i - 1][j][t];
+          // E^{i-1,j}_t vanishes for t > i-1+j: that entry was never written, read it as 0
+          v = (t <= i - 1 + j) ? xpa * E[i - 1][j][t] : 0.0;
           if (t > 0) v += h * E[i - 1][j][t - 1];
           if (t + 1 <= i - 1 + j) v += (t + 1) * E[i - 1][j][t + 1];
         } else {
-          v = xpb * E[i][j - 1][t];
+          v = (t <= i + j - 1) ? xpb * E[i][j - 1][t] : 0.0;
           if (t > 0) v += h * E[i][j - 1][t - 1];
           if (t + 1 <= i + j - 1) v += (t + 1) * E[i][j - 1][t + 1];
         }
@@ -1863,4 +1864,483 @@ extern "C" int sqb200_syev_batched(int device, int n, int batch, double* A, doub
     return fail(SQB200_ECUDA, "cusolverDnXsyevBatched failed");
   CUDA_OK(cudaGetLastError());
   return SQB200_OK;
+}
+
+// ---------------------------------------------------------------- nuclear gradient
+//
+// Gradient of the SCF energy with respect to the nuclear positions, as uhf_force computes it
+// (src/grad.c:2155-2420; the forces are its negative): nuclear repulsion, -sum W dS (W the
+// energy-weighted density), sum PT d(T + V) including the Hellmann-Feynman term of each
+// nucleus, and the two-electron term of GradEri_ShellSet_Parallel (src/grad.c:1734):
+// sum over unique shell quartets of Gamma_abcd d(ab|cd), with
+// Gamma = deg * [4 PT_ab PT_cd - (PT_ac PT_bd + PT_ad PT_bc + PS_ac PS_bd + PS_ad PS_bc)]
+// (the reference's 0.5 PT PT - 0.25 (PT PT + PS PS) summed over the eight index permutations),
+// shell quartets skipped when Sch(PQ) Sch(IJ) maxPT(PQ) maxPT(IJ) < 1e-10, primitive quartets
+// below the 1e-15 prefactor cut, and, as the reference does, a function quartet of a primitive
+// quartet whose density factor times prefactor and weights is below 1e-10.  Derivatives of a primitive by its centre raise and lower
+// its angular momentum, d/dA_x g_a = 2 alpha g_{a+1x} - a_x g_{a-1x}; the fourth centre follows
+// from translational invariance.  The integrals are McMurchie-Davidson with runtime loops (one
+// thread per shell quartet or function pair): a correctness-first form, not tuned.
+
+namespace {
+
+struct GShell {
+  int first, nfunc, nprim, poff;   // poff: first primitive in the exps / wts arrays
+  int lmax, atom;
+  double x, y, z;
+  int lmn[6][3];
+};
+
+#define GR_MAXL 9                  // highest Hermite order: (dd|dd) + 1
+#define GR_NT 220                  // tetra(GR_MAXL) entries
+
+// F_0..F_M (M <= 9, runtime) from the same grid as boys<M>: the top order by the Taylor
+// expansion with as many terms as the table's columns allow, then downward recursion.
+__device__ void boys_rt(int M, double T, const double* __restrict__ tab, double* F) {
+  if (T < BOYS_TMAX) {
+    const int g = __double2int_rn(T * BOYS_INV_H);
+    const double d = T - g * BOYS_H;
+    const double* row = tab + g * BOYS_NCOL + M;
+    const int nt = min(BOYS_NTAY, BOYS_NCOL - M);
+    double s = row[nt - 1];
+    for (int k = nt - 2; k >= 0; --k) s = fma(s, -d * (1.0 / (double)(k + 1)), row[k]);
+    F[M] = s;
+    if (M > 0) {
+      const double e = exp(-T);
+      for (int m = M - 1; m >= 0; --m) F[m] = (2.0 * T * F[m + 1] + e) / (2 * m + 1);
+    }
+  } else {
+    F[0] = 0.5 * sqrt(M_PI / T);
+    const double e = exp(-T);
+    for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2.0 * T);
+  }
+}
+
+// 1-D Hermite expansion coefficients E^{ij}_t, i <= imax, j <= jmax (prefactor excluded)
+template <int NI, int NJ, int NT>
+__device__ void herm1d(double p, double xpa, double xpb, int imax, int jmax, double E[NI][NJ][NT]) {
+  const double h = 0.5 / p;
+  for (int i = 0; i <= imax; ++i)
+    for (int j = 0; j <= jmax; ++j)
+      for (int t = 0; t <= i + j; ++t) {
+        double v;
+        if (i == 0 && j == 0) v = (t == 0) ? 1.0 : 0.0;
+        else if (i > 0) {
+          // E^{i-1,j}_t vanishes for t > i-1+j: that entry was never written, read it as 0
+          v = (t <= i - 1 + j) ? xpa * E[i - 1][j][t] : 0.0;
+          if (t > 0) v += h * E[i - 1][j][t - 1];
+          if (t + 1 <= i - 1 + j) v += (t + 1) * E[i - 1][j][t + 1];
+        } else {
+          v = (t <= i + j - 1) ? xpb * E[i][j - 1][t] : 0.0;
+          if (t > 0) v += h * E[i][j - 1][t - 1];
+          if (t + 1 <= i + j - 1) v += (t + 1) * E[i][j - 1][t + 1];
+        }
+        E[i][j][t] = v;
+      }
+}
+
+// R_tuv (order 0) for t+u+v <= L into R (tetra index), from base[n] = (-2 a)^n F_n
+__device__ void herm_R(int L, double a, double X, double Y, double Z, const double* F, double* R, double* tmp) {
+  double base[GR_MAXL + 1];
+  double w = 1.0;
+  for (int n = 0; n <= L; ++n) { base[n] = w * F[n]; w *= -2.0 * a; }
+  double* cur = (L % 2 == 0) ? R : tmp;
+  double* nxt = (L % 2 == 0) ? tmp : R;
+  cur[0] = base[L];
+  for (int n = L - 1; n >= 0; --n) {
+    for (int N = 0; N <= L - n; ++N)
+      for (int t = N; t >= 0; --t)
+        for (int u = N - t; u >= 0; --u) {
+          const int v = N - t - u;
+          double r;
+          if (N == 0) r = base[n];
+          else if (t > 0) r = X * cur[tetra(t - 1, u, v)] + (t > 1 ? (t - 1) * cur[tetra(t - 2, u, v)] : 0.0);
+          else if (u > 0) r = Y * cur[tetra(t, u - 1, v)] + (u > 1 ? (u - 1) * cur[tetra(t, u - 2, v)] : 0.0);
+          else r = Z * cur[tetra(t, u, v - 1)] + (v > 1 ? (v - 1) * cur[tetra(t, u, v - 2)] : 0.0);
+          nxt[tetra(t, u, v)] = r;
+        }
+    double* s = cur; cur = nxt; nxt = s;
+  }
+}
+
+// d/dA of a 1-D factor: 2 alpha f(i+1) - i f(i-1)
+__device__ __forceinline__ double draise(double two_alpha, int i, double up, double down) {
+  return two_alpha * up - (i > 0 ? i * down : 0.0);
+}
+
+__global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const double* __restrict__ psch,
+                           const double* __restrict__ ppm, const GShell* __restrict__ shells,
+                           const double* __restrict__ exps, const double* __restrict__ wts,
+                           const double* __restrict__ PT, const double* __restrict__ PS, int nbf,
+                           const double* __restrict__ tab, double* __restrict__ grad) {
+  const int pq = blockIdx.y;
+  const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pq >= npairs || ij > pq) return;
+  if (psch[pq] * psch[ij] * ppm[pq] * ppm[ij] < 1e-10) return;
+  const int2 PQ = pairs[pq], IJ = pairs[ij];
+  const GShell A = shells[PQ.x], B = shells[PQ.y], C = shells[IJ.x], D = shells[IJ.y];
+  const double deg = (PQ.x == PQ.y ? 0.5 : 1.0) * (IJ.x == IJ.y ? 0.5 : 1.0) * (pq == ij ? 0.5 : 1.0);
+  const int Lb = A.lmax + B.lmax + 1, L = A.lmax + B.lmax + C.lmax + D.lmax + 1;
+  double g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  double Eb[3][4][4][8], Ek[3][4][4][8];
+  double F[GR_MAXL + 1], R[GR_NT], tmp[GR_NT], V[4][56];
+  const double ab2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
+  const double cd2 = (C.x - D.x) * (C.x - D.x) + (C.y - D.y) * (C.y - D.y) + (C.z - D.z) * (C.z - D.z);
+  for (int ka = 0; ka < A.nprim; ++ka)
+    for (int kb = 0; kb < B.nprim; ++kb) {
+      const double ea = exps[A.poff + ka], eb = exps[B.poff + kb], p = ea + eb;
+      const double Px = (ea * A.x + eb * B.x) / p, Py = (ea * A.y + eb * B.y) / p, Pz = (ea * A.z + eb * B.z) / p;
+      const double Kab = exp(-ea * eb / p * ab2);
+      herm1d<4, 4, 8>(p, Px - A.x, Px - B.x, A.lmax + 1, B.lmax + 1, Eb[0]);
+      herm1d<4, 4, 8>(p, Py - A.y, Py - B.y, A.lmax + 1, B.lmax + 1, Eb[1]);
+      herm1d<4, 4, 8>(p, Pz - A.z, Pz - B.z, A.lmax + 1, B.lmax + 1, Eb[2]);
+      for (int kc = 0; kc < C.nprim; ++kc)
+        for (int kd = 0; kd < D.nprim; ++kd) {
+          const double ec = exps[C.poff + kc], ed = exps[D.poff + kd], q = ec + ed;
+          const double Kcd = exp(-ec * ed / q * cd2);
+          const double pre = TWO_PI_2_5 * Kab * Kcd / (p * q * sqrt(p + q));
+          if (pre < PRIM_CUTOFF) continue;
+          const double Qx = (ec * C.x + ed * D.x) / q, Qy = (ec * C.y + ed * D.y) / q, Qz = (ec * C.z + ed * D.z) / q;
+          herm1d<4, 4, 8>(q, Qx - C.x, Qx - D.x, C.lmax + 1, D.lmax, Ek[0]);
+          herm1d<4, 4, 8>(q, Qy - C.y, Qy - D.y, C.lmax + 1, D.lmax, Ek[1]);
+          herm1d<4, 4, 8>(q, Qz - C.z, Qz - D.z, C.lmax + 1, D.lmax, Ek[2]);
+          const double al = p * q / (p + q);
+          const double X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;
+          boys_rt(L, al * (X * X + Y * Y + Z * Z), tab, F);
+          herm_R(L, al, X, Y, Z, F, R, tmp);
+          for (int c = 0; c < C.nfunc; ++c)
+            for (int d = 0; d < D.nfunc; ++d) {
+              const int* lc = C.lmn[c];
+              const int* ld = D.lmn[d];
+              const double wcd = wts[(C.poff + kc) * 6 + c] * wts[(D.poff + kd) * 6 + d];
+              if (wcd == 0.0) continue;
+              // V0 = sum_k (-1)^k E^cd_k R_{h+k}; V1..3 the same with d/dC_{x,y,z} E^cd
+              for (int N = 0; N <= Lb; ++N)
+                for (int t = N; t >= 0; --t)
+                  for (int u = N - t; u >= 0; --u) {
+                    const int v = N - t - u, hi = tetra(t, u, v);
+                    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+                    for (int tt = 0; tt <= lc[0] + 1 + ld[0]; ++tt)
+                      for (int uu = 0; uu <= lc[1] + 1 + ld[1]; ++uu)
+                        for (int vv = 0; vv <= lc[2] + 1 + ld[2]; ++vv) {
+                          // R is computed up to order L; the terms beyond it pair a raised bra
+                          // index with a raised ket index, which no derivative uses
+                          if (N + tt + uu + vv > L) continue;
+                          const double r = ((tt + uu + vv) & 1 ? -1.0 : 1.0) * R[tetra(t + tt, u + uu, v + vv)];
+                          const bool bx = tt <= lc[0] + ld[0], by = uu <= lc[1] + ld[1], bz = vv <= lc[2] + ld[2];
+                          const double ex = bx ? Ek[0][lc[0]][ld[0]][tt] : 0.0;
+                          const double ey = by ? Ek[1][lc[1]][ld[1]][uu] : 0.0;
+                          const double ez = bz ? Ek[2][lc[2]][ld[2]][vv] : 0.0;
+                          const double dx = draise(2 * ec, lc[0], Ek[0][lc[0] + 1][ld[0]][tt],
+                                                   lc[0] > 0 && tt <= lc[0] - 1 + ld[0] ? Ek[0][lc[0] - 1][ld[0]][tt] : 0.0);
+                          const double dy = draise(2 * ec, lc[1], Ek[1][lc[1] + 1][ld[1]][uu],
+                                                   lc[1] > 0 && uu <= lc[1] - 1 + ld[1] ? Ek[1][lc[1] - 1][ld[1]][uu] : 0.0);
+                          const double dz = draise(2 * ec, lc[2], Ek[2][lc[2] + 1][ld[2]][vv],
+                                                   lc[2] > 0 && vv <= lc[2] - 1 + ld[2] ? Ek[2][lc[2] - 1][ld[2]][vv] : 0.0);
+                          s0 += ex * ey * ez * r;
+                          s1 += dx * ey * ez * r;
+                          s2 += ex * dy * ez * r;
+                          s3 += ex * ey * dz * r;
+                        }
+                    V[0][hi] = s0; V[1][hi] = s1; V[2][hi] = s2; V[3][hi] = s3;
+                  }
+              const int fc = C.first + c, fd = D.first + d;
+              for (int a = 0; a < A.nfunc; ++a)
+                for (int b = 0; b < B.nfunc; ++b) {
+                  const int fa = A.first + a, fb = B.first + b;
+                  const double gam = 4.0 * PT[fa * nbf + fb] * PT[fc * nbf + fd] -
+                                     (PT[fa * nbf + fc] * PT[fb * nbf + fd] + PT[fa * nbf + fd] * PT[fb * nbf + fc] +
+                                      PS[fa * nbf + fc] * PS[fb * nbf + fd] + PS[fa * nbf + fd] * PS[fb * nbf + fc]);
+                  const double wab = wts[(A.poff + ka) * 6 + a] * wts[(B.poff + kb) * 6 + b];
+                  // the reference's per-primitive screen of one function quartet
+                  // (src/grad.c:1982-1988): |coef r| < 1e-10, coef its density factor with the
+                  // function-level degeneracy, r the primitive prefactor times the four weights
+                  const double dfn = (fa == fb ? 0.5 : 1.0) * (fc == fd ? 0.5 : 1.0) *
+                                     ((fa == fc && fb == fd) || (fa == fd && fb == fc) ? 0.5 : 1.0);
+                  if (fabs(gam * dfn * pre * wab * wcd) < 1e-10) continue;
+                  const double G = deg * pre * wcd * wab * gam;
+                  if (G == 0.0) continue;
+                  const int* la = A.lmn[a];
+                  const int* lb = B.lmn[b];
+                  double dA[3] = {0, 0, 0}, dB[3] = {0, 0, 0}, dC[3] = {0, 0, 0};
+                  for (int t = 0; t <= la[0] + lb[0] + 1; ++t)
+                    for (int u = 0; u <= la[1] + lb[1] + 1; ++u)
+                      for (int v = 0; v <= la[2] + lb[2] + 1; ++v) {
+                        if (t + u + v > Lb) continue;
+                        const int hi = tetra(t, u, v);
+                        const bool bx = t <= la[0] + lb[0], by = u <= la[1] + lb[1], bz = v <= la[2] + lb[2];
+                        const double ex = bx ? Eb[0][la[0]][lb[0]][t] : 0.0;
+                        const double ey = by ? Eb[1][la[1]][lb[1]][u] : 0.0;
+                        const double ez = bz ? Eb[2][la[2]][lb[2]][v] : 0.0;
+                        const double ax = draise(2 * ea, la[0], Eb[0][la[0] + 1][lb[0]][t],
+                                                 la[0] > 0 && t <= la[0] - 1 + lb[0] ? Eb[0][la[0] - 1][lb[0]][t] : 0.0);
+                        const double ay = draise(2 * ea, la[1], Eb[1][la[1] + 1][lb[1]][u],
+                                                 la[1] > 0 && u <= la[1] - 1 + lb[1] ? Eb[1][la[1] - 1][lb[1]][u] : 0.0);
+                        const double az = draise(2 * ea, la[2], Eb[2][la[2] + 1][lb[2]][v],
+                                                 la[2] > 0 && v <= la[2] - 1 + lb[2] ? Eb[2][la[2] - 1][lb[2]][v] : 0.0);
+                        const double bxd = draise(2 * eb, lb[0], Eb[0][la[0]][lb[0] + 1][t],
+                                                  lb[0] > 0 && t <= la[0] + lb[0] - 1 ? Eb[0][la[0]][lb[0] - 1][t] : 0.0);
+                        const double byd = draise(2 * eb, lb[1], Eb[1][la[1]][lb[1] + 1][u],
+                                                  lb[1] > 0 && u <= la[1] + lb[1] - 1 ? Eb[1][la[1]][lb[1] - 1][u] : 0.0);
+                        const double bzd = draise(2 * eb, lb[2], Eb[2][la[2]][lb[2] + 1][v],
+                                                  lb[2] > 0 && v <= la[2] + lb[2] - 1 ? Eb[2][la[2]][lb[2] - 1][v] : 0.0);
+                        const double v0 = V[0][hi];
+                        dA[0] += ax * ey * ez * v0;
+                        dA[1] += ex * ay * ez * v0;
+                        dA[2] += ex * ey * az * v0;
+                        dB[0] += bxd * ey * ez * v0;
+                        dB[1] += ex * byd * ez * v0;
+                        dB[2] += ex * ey * bzd * v0;
+                        const double e3 = ex * ey * ez;
+                        dC[0] += e3 * V[1][hi];
+                        dC[1] += e3 * V[2][hi];
+                        dC[2] += e3 * V[3][hi];
+                      }
+                  for (int x = 0; x < 3; ++x) {
+                    g[0][x] += G * dA[x];
+                    g[1][x] += G * dB[x];
+                    g[2][x] += G * dC[x];
+                  }
+                }
+            }
+        }
+    }
+  for (int x = 0; x < 3; ++x) {
+    atomicAdd(grad + 3 * A.atom + x, g[0][x]);
+    atomicAdd(grad + 3 * B.atom + x, g[1][x]);
+    atomicAdd(grad + 3 * C.atom + x, g[2][x]);
+    atomicAdd(grad + 3 * D.atom + x, -(g[0][x] + g[1][x] + g[2][x]));
+  }
+}
+
+}  // namespace
+
+namespace {
+
+// One-electron part of the gradient, one thread per ordered function pair (a, b):
+// -W_ab dS_ab, PT_ab d(T_ab + V_ab) on the atoms of a and b, and the Hellmann-Feynman term
+// PT_ab dV^C_ab / dC = -PT_ab (dV^C/dA + dV^C/dB) on every nucleus C.
+__global__ void k_grad_1e(int nbf, const int* __restrict__ nprim, const int* __restrict__ off,
+                          const int* __restrict__ lmn, const double* __restrict__ xyz,
+                          const double* __restrict__ exps, const double* __restrict__ nc,
+                          const int* __restrict__ fatom, int natom, const double* __restrict__ Z,
+                          const double* __restrict__ axyz, const double* __restrict__ tab,
+                          const double* __restrict__ PT, const double* __restrict__ W, double* __restrict__ grad,
+                          int terms) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nbf * nbf) return;
+  const int ia = idx / nbf, ib = idx % nbf;
+  const double pt = (terms & SQB200_GRAD_HCORE) ? PT[idx] : 0.0;
+  const double w = (terms & SQB200_GRAD_OVERLAP) ? W[idx] : 0.0;
+  if (pt == 0.0 && w == 0.0) return;
+  const int* la = lmn + 3 * ia;
+  const int* lb = lmn + 3 * ib;
+  const double* A = xyz + 3 * ia;
+  const double* B = xyz + 3 * ib;
+  double E[3][4][5][8];
+  double F[GR_MAXL + 1], R[GR_NT], tmp[GR_NT];
+  double gA[3] = {0, 0, 0};      // d/dA of PT (T + V) - W S (the B side is added by translational invariance)
+  double gB[3] = {0, 0, 0};      // d/dB of PT V (kinetic and overlap: -d/dA)
+  const double ab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
+  const int L = la[0] + la[1] + la[2] + lb[0] + lb[1] + lb[2] + 1;
+  for (int i = 0; i < nprim[ia]; ++i)
+    for (int j = 0; j < nprim[ib]; ++j) {
+      const double a = exps[off[ia] + i], b = exps[off[ib] + j], p = a + b;
+      const double c = nc[off[ia] + i] * nc[off[ib] + j] * exp(-a * b * ab2 / p);
+      const double P[3] = {(a * A[0] + b * B[0]) / p, (a * A[1] + b * B[1]) / p, (a * A[2] + b * B[2]) / p};
+      for (int d = 0; d < 3; ++d) herm1d<4, 5, 8>(p, P[d] - A[d], P[d] - B[d], la[d] + 1, lb[d] + 2, E[d]);
+      const double sq = sqrt(M_PI / p);
+      // 1-D overlap S(i,j) and kinetic T(i,j) factors and their d/dA
+      double S0[3], T0[3], dS[3], dT[3];
+      for (int d = 0; d < 3; ++d) {
+        const int ii = la[d], jj = lb[d];
+        auto Sf = [&](int i2, int j2) { return (i2 < 0 || j2 < 0) ? 0.0 : E[d][i2][j2][0] * sq; };
+        auto Tf = [&](int i2, int j2) {
+          if (i2 < 0) return 0.0;
+          double k = -2.0 * b * (2 * j2 + 1) * Sf(i2, j2) + 4.0 * b * b * Sf(i2, j2 + 2);
+          if (j2 >= 2) k += j2 * (j2 - 1) * Sf(i2, j2 - 2);
+          return -0.5 * k;
+        };
+        S0[d] = Sf(ii, jj);
+        T0[d] = Tf(ii, jj);
+        dS[d] = draise(2 * a, ii, Sf(ii + 1, jj), Sf(ii - 1, jj));
+        dT[d] = draise(2 * a, ii, Tf(ii + 1, jj), Tf(ii - 1, jj));
+      }
+      for (int x = 0; x < 3; ++x) {
+        const int y = (x + 1) % 3, z = (x + 2) % 3;
+        const double dSab = dS[x] * S0[y] * S0[z];
+        const double dTab = dT[x] * S0[y] * S0[z] + dS[x] * (T0[y] * S0[z] + S0[y] * T0[z]);
+        gA[x] += c * (pt * dTab - w * dSab);
+        gB[x] -= c * (pt * dTab - w * dSab);
+      }
+      // nuclear attraction: V^C = -Z_C (2 pi / p) sum_tuv E^ab_tuv R_tuv(p, P - C)
+      for (int at = 0; at < natom; ++at) {
+        const double X = P[0] - axyz[3 * at], Y = P[1] - axyz[3 * at + 1], Zc = P[2] - axyz[3 * at + 2];
+        boys_rt(L, p * (X * X + Y * Y + Zc * Zc), tab, F);
+        herm_R(L, p, X, Y, Zc, F, R, tmp);
+        const double f = -Z[at] * (2.0 * M_PI / p) * c * pt;
+        double vA[3] = {0, 0, 0}, vB[3] = {0, 0, 0};
+        for (int t = 0; t <= la[0] + lb[0] + 1; ++t)
+          for (int u = 0; u <= la[1] + lb[1] + 1; ++u)
+            for (int v = 0; v <= la[2] + lb[2] + 1; ++v) {
+              if (t + u + v > L) continue;
+              const double r = R[tetra(t, u, v)];
+              const double ex = t <= la[0] + lb[0] ? E[0][la[0]][lb[0]][t] : 0.0;
+              const double ey = u <= la[1] + lb[1] ? E[1][la[1]][lb[1]][u] : 0.0;
+              const double ez = v <= la[2] + lb[2] ? E[2][la[2]][lb[2]][v] : 0.0;
+              const double ax = draise(2 * a, la[0], E[0][la[0] + 1][lb[0]][t], la[0] > 0 && t <= la[0] - 1 + lb[0] ? E[0][la[0] - 1][lb[0]][t] : 0.0);
+              const double ay = draise(2 * a, la[1], E[1][la[1] + 1][lb[1]][u], la[1] > 0 && u <= la[1] - 1 + lb[1] ? E[1][la[1] - 1][lb[1]][u] : 0.0);
+              const double az = draise(2 * a, la[2], E[2][la[2] + 1][lb[2]][v], la[2] > 0 && v <= la[2] - 1 + lb[2] ? E[2][la[2] - 1][lb[2]][v] : 0.0);
+              const double bx = draise(2 * b, lb[0], E[0][la[0]][lb[0] + 1][t], lb[0] > 0 && t <= la[0] + lb[0] - 1 ? E[0][la[0]][lb[0] - 1][t] : 0.0);
+              const double by = draise(2 * b, lb[1], E[1][la[1]][lb[1] + 1][u], lb[1] > 0 && u <= la[1] + lb[1] - 1 ? E[1][la[1]][lb[1] - 1][u] : 0.0);
+              const double bz = draise(2 * b, lb[2], E[2][la[2]][lb[2] + 1][v], lb[2] > 0 && v <= la[2] + lb[2] - 1 ? E[2][la[2]][lb[2] - 1][v] : 0.0);
+              vA[0] += ax * ey * ez * r; vA[1] += ex * ay * ez * r; vA[2] += ex * ey * az * r;
+              vB[0] += bx * ey * ez * r; vB[1] += ex * by * ez * r; vB[2] += ex * ey * bz * r;
+            }
+        for (int x = 0; x < 3; ++x) {
+          gA[x] += f * vA[x];
+          gB[x] += f * vB[x];
+          atomicAdd(grad + 3 * at + x, -f * (vA[x] + vB[x]));
+        }
+      }
+    }
+  for (int x = 0; x < 3; ++x) {
+    atomicAdd(grad + 3 * fatom[ia] + x, gA[x]);
+    atomicAdd(grad + 3 * fatom[ib] + x, gB[x]);
+  }
+}
+
+}  // namespace
+
+extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, const double* axyz,
+                                     const double* PA, const double* PB, const double* W, int terms, double* grad) {
+  if (!c || natom <= 0 || !Z || !axyz || !PA || !PB || !W || !grad) return fail(SQB200_EINVAL, "null argument");
+  CUDA_OK(cudaSetDevice(c->device));
+  const int n = c->nbf;
+  const size_t nn = (size_t)n * n;
+  // functions: primitive data, atom (the centre the basis function sits on)
+  std::vector<int> np(n), off(n), lmn(3 * n), fat(n, -1);
+  std::vector<double> xyz(3 * n), ex, nc;
+  for (const Shell& sh : c->shells)
+    for (int f = 0; f < sh.nfunc; ++f) {
+      const int q = sh.first + f;
+      np[q] = sh.nprim;
+      off[q] = (int)ex.size();
+      for (int d = 0; d < 3; ++d) lmn[3 * q + d] = sh.lmn[f][d];
+      xyz[3 * q] = sh.x; xyz[3 * q + 1] = sh.y; xyz[3 * q + 2] = sh.z;
+      for (int k = 0; k < sh.nprim; ++k) { ex.push_back(sh.exps[k]); nc.push_back(sh.coef[k][f]); }
+    }
+  auto atom_of = [&](double x, double y, double z) {
+    for (int a = 0; a < natom; ++a)
+      if (fabs(axyz[3 * a] - x) < 1e-8 && fabs(axyz[3 * a + 1] - y) < 1e-8 && fabs(axyz[3 * a + 2] - z) < 1e-8) return a;
+    return -1;
+  };
+  for (int q = 0; q < n; ++q) {
+    fat[q] = atom_of(xyz[3 * q], xyz[3 * q + 1], xyz[3 * q + 2]);
+    if (fat[q] < 0) return fail(SQB200_EINVAL, "sqb200_gradient: a basis function is not centred on an atom");
+  }
+  // shells, shell-major primitive weights (6 functions per primitive row)
+  const int ns = (int)c->shells.size();
+  std::vector<GShell> gs(ns);
+  std::vector<double> sex, swt;
+  for (int s = 0; s < ns; ++s) {
+    const Shell& sh = c->shells[s];
+    GShell& g = gs[s];
+    g.first = sh.first; g.nfunc = sh.nfunc; g.nprim = sh.nprim; g.poff = (int)sex.size();
+    g.lmax = 0;
+    for (int f = 0; f < sh.nfunc; ++f) {
+      for (int d = 0; d < 3; ++d) g.lmn[f][d] = sh.lmn[f][d];
+      g.lmax = std::max(g.lmax, sh.lmn[f][0] + sh.lmn[f][1] + sh.lmn[f][2]);
+    }
+    if (g.lmax > 2) return fail(SQB200_EUNSUPPORTED, "sqb200_gradient: shells beyond d");
+    g.atom = fat[sh.first]; g.x = sh.x; g.y = sh.y; g.z = sh.z;
+    for (int k = 0; k < sh.nprim; ++k) {
+      sex.push_back(sh.exps[k]);
+      for (int f = 0; f < 6; ++f) swt.push_back(f < sh.nfunc ? sh.coef[k][f] : 0.0);
+    }
+  }
+  // shell pairs P >= Q with their Schwarz and |PT| block maxima
+  std::vector<int2> pairs;
+  std::vector<double> psch, ppm;
+  for (int P = 0; P < ns; ++P)
+    for (int Q = 0; Q <= P; ++Q) {
+      double sm = 0.0, pm = 0.0;
+      for (int p = 0; p < c->shells[P].nfunc; ++p)
+        for (int q = 0; q < c->shells[Q].nfunc; ++q) {
+          const size_t e = (size_t)(c->shells[P].first + p) * n + c->shells[Q].first + q;
+          sm = std::max(sm, c->schwarz[e]);
+          pm = std::max(pm, fabs(PA[e] + PB[e]));
+        }
+      pairs.push_back(make_int2(P, Q));
+      psch.push_back(sm);
+      ppm.push_back(pm);
+    }
+  const int npairs = (int)pairs.size();
+  if (npairs > 65535) return fail(SQB200_EINVAL, "sqb200_gradient: more than 65535 shell pairs");
+  std::vector<double> PT(nn), PS(nn);
+  for (size_t i = 0; i < nn; ++i) { PT[i] = PA[i] + PB[i]; PS[i] = PA[i] - PB[i]; }
+  void* d[16] = {nullptr};
+  auto up = [&](int k, const void* h, size_t bytes) -> cudaError_t {
+    cudaError_t e = cudaMalloc(&d[k], bytes ? bytes : 8);
+    if (e == cudaSuccess && bytes) e = cudaMemcpy(d[k], h, bytes, cudaMemcpyHostToDevice);
+    return e;
+  };
+  cudaError_t e = up(0, np.data(), n * sizeof(int));
+  if (e == cudaSuccess) e = up(1, off.data(), n * sizeof(int));
+  if (e == cudaSuccess) e = up(2, lmn.data(), 3 * n * sizeof(int));
+  if (e == cudaSuccess) e = up(3, xyz.data(), 3 * n * sizeof(double));
+  if (e == cudaSuccess) e = up(4, ex.data(), ex.size() * sizeof(double));
+  if (e == cudaSuccess) e = up(5, nc.data(), nc.size() * sizeof(double));
+  if (e == cudaSuccess) e = up(6, fat.data(), n * sizeof(int));
+  if (e == cudaSuccess) e = up(7, Z, natom * sizeof(double));
+  if (e == cudaSuccess) e = up(8, axyz, 3 * natom * sizeof(double));
+  if (e == cudaSuccess) e = up(9, PT.data(), nn * sizeof(double));
+  if (e == cudaSuccess) e = up(10, PS.data(), nn * sizeof(double));
+  if (e == cudaSuccess) e = up(11, W, nn * sizeof(double));
+  if (e == cudaSuccess) e = up(12, gs.data(), ns * sizeof(GShell));
+  if (e == cudaSuccess) e = up(13, sex.data(), sex.size() * sizeof(double));
+  if (e == cudaSuccess) e = up(14, swt.data(), swt.size() * sizeof(double));
+  if (e == cudaSuccess) e = up(15, nullptr, 0);
+  void* dp = nullptr;
+  void *dsch = nullptr, *dpm = nullptr, *dg = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&dp, npairs * sizeof(int2));
+  if (e == cudaSuccess) e = cudaMemcpy(dp, pairs.data(), npairs * sizeof(int2), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&dsch, npairs * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(dsch, psch.data(), npairs * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&dpm, npairs * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(dpm, ppm.data(), npairs * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&dg, 3 * natom * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, 3 * natom * sizeof(double), c->stream);
+  if (e == cudaSuccess) {
+    if (terms & SQB200_GRAD_ERI)
+      k_grad_eri<<<dim3((npairs + 127) / 128, npairs), 128, 0, c->stream>>>(
+          npairs, (const int2*)dp, (const double*)dsch, (const double*)dpm, (const GShell*)d[12], (const double*)d[13],
+          (const double*)d[14], (const double*)d[9], (const double*)d[10], n, c->d_boys, (double*)dg);
+    if (terms & (SQB200_GRAD_HCORE | SQB200_GRAD_OVERLAP))
+      k_grad_1e<<<(int)((nn + 127) / 128), 128, 0, c->stream>>>(
+          n, (const int*)d[0], (const int*)d[1], (const int*)d[2], (const double*)d[3], (const double*)d[4],
+          (const double*)d[5], (const int*)d[6], natom, (const double*)d[7], (const double*)d[8], c->d_boys,
+          (const double*)d[9], (const double*)d[11], (double*)dg, terms);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(grad, dg, 3 * natom * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  for (void* q : d) cudaFree(q);
+  cudaFree(dp); cudaFree(dsch); cudaFree(dpm); cudaFree(dg);
+  if (e != cudaSuccess) return fail(SQB200_ECUDA, std::string("sqb200_gradient: ") + cudaGetErrorString(e));
+  // nuclear repulsion (GradVnn, src/grad.c:43)
+  if (terms & SQB200_GRAD_NUCLEAR)
+  for (int i = 0; i < natom; ++i)
+    for (int j = 0; j < natom; ++j) {
+      if (i == j) continue;
+      const double dx = axyz[3 * i] - axyz[3 * j], dy = axyz[3 * i + 1] - axyz[3 * j + 1], dz = axyz[3 * i + 2] - axyz[3 * j + 2];
+      const double r = sqrt(dx * dx + dy * dy + dz * dz), f = -Z[i] * Z[j] / (r * r * r);
+      grad[3 * i] += f * dx; grad[3 * i + 1] += f * dy; grad[3 * i + 2] += f * dz;
+    }
+  return SQB200_OK;
+}
+
+extern "C" int sqb200_gradient(sqb200_jk* c, int natom, const double* Z, const double* axyz, const double* PA,
+                               const double* PB, const double* W, double* grad) {
+  return sqb200_gradient_terms(c, natom, Z, axyz, PA, PB, W, SQB200_GRAD_ALL, grad);
 }

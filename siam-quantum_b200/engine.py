@@ -26,7 +26,7 @@ EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_j
            "sqb200_peak_fma", "sqb200_batch_create", "sqb200_batch_destroy", "sqb200_batch_offsets",
            "sqb200_batch_set_step", "sqb200_batch_build_device", "sqb200_batch_stats",
            "sqb200_batch_autotune", "sqb200_jk_autotune", "sqb200_jk_tiles", "sqb200_jk_set_tiles",
-           "sqb200_syev_batched",
+           "sqb200_syev_batched", "sqb200_gradient", "sqb200_gradient_terms",
            "sqb200_last_error"]
 
 
@@ -71,6 +71,8 @@ def load_library(path=LIB_PATH):
                                      ctypes.c_double, vp]
     L.sqb200_jk_tiles.argtypes = [vp, _i32p, ctypes.c_int]
     L.sqb200_syev_batched.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
+    L.sqb200_gradient.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
+    L.sqb200_gradient_terms.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_int, _f64p]
     L.sqb200_jk_set_tiles.argtypes = [vp, _i32p, ctypes.c_int]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
@@ -219,6 +221,16 @@ class JKEngine:
         _check(_lib.sqb200_oneint(self._ctx, len(Z), Z if len(Z) else np.zeros(1),
                                   A if len(A) else np.zeros(3), S, T, V))
         return S.reshape(n, n), T.reshape(n, n), V.reshape(n, n)
+
+    def gradient(self, charges, coords_bohr, PA, PB, W, terms=15):
+        """Nuclear gradient (natom, 3) in hartree/bohr (sqb200_gradient_terms; terms: bits
+        1 nuclear repulsion, 2 PT d(T+V), 4 -W dS, 8 two-electron)."""
+        Z = np.ascontiguousarray(charges, dtype=np.float64).reshape(-1)
+        A = np.ascontiguousarray(coords_bohr, dtype=np.float64).reshape(-1)
+        f = lambda m: np.ascontiguousarray(m, dtype=np.float64).reshape(-1)
+        g = np.zeros(3 * len(Z))
+        _check(_lib.sqb200_gradient_terms(self._ctx, len(Z), Z, A, f(PA), f(PB), f(W), int(terms), g))
+        return g.reshape(-1, 3)
 
     def mem_cutoff(self, fixed_cutoff, max_mem_mb):
         v = ctypes.c_double()

@@ -289,6 +289,19 @@ class SCFJob:
             out.append((C.cpu().numpy(), w.cpu().numpy()))
         return out[0][0], out[1][0], out[0][1], out[1][1]
 
+    def gradient(self, terms=15):
+        """Nuclear gradient (natom, 3), hartree/bohr, of the converged SCF energy, as the
+        reference's uhf_force (src/grad.c:2155) forms it after uhf(): densities and the
+        energy-weighted density from the orbitals of the last Fock matrices."""
+        CA, CB, eA, eB = self.orbitals()
+        ca, cb = CA[:self.nea], CB[:self.neb]
+        PA = ca.T @ ca
+        PB = cb.T @ cb
+        W = (ca.T * eA[:self.nea]) @ ca + (cb.T * eB[:self.neb]) @ cb
+        Z = np.array([a[0] for a in self.atoms], dtype=np.float64)
+        XYZ = np.array([a[1:] for a in self.atoms], dtype=np.float64)
+        return self.eng.gradient(Z, XYZ, PA, PB, W, terms)
+
     def save_checkpoint(self, path):
         """Write the reference's checkpoint file (-SCHECK) for this job."""
         from . import checkpoint as CK

@@ -14,6 +14,7 @@ seeded synthetic molecules and stores, per case, in <case>.npz:
 Usage:  make -C oracle && python tests/golden/make_golden.py
         python tests/golden/make_golden.py --oneint   (add S, T, V to existing fixtures only)
         python tests/golden/make_golden.py --iters    (add the reference's SCF iteration count)
+        python tests/golden/make_golden.py --forces   (add the reference's forces, uhf_force)
 """
 import os
 import subprocess
@@ -112,6 +113,22 @@ def add_scf_iters():
         print(name, "reference SCF iterations", res["iters"])
 
 
+def add_forces():
+    """Store the reference's forces (uhf_force after uhf(), 1STEP, SCFConv 1e-8)."""
+    for name, geom, bas, opts in CASES:
+        path = os.path.join(OUT, name + ".npz")
+        rec = dict(np.load(path, allow_pickle=True))
+        with tempfile.TemporaryDirectory() as d:
+            xyz = os.path.join(d, "m.xyz")
+            with open(xyz, "w") as f:
+                f.write(M.xyz_text(geom(), name))
+            F, res = port.ref_force(xyz, os.path.join(BASIS_DIR, bas + ".txt"),
+                                    ["-SCFACC=1STEP", "-SCFCONV=1e-8"] + list(opts))
+        rec["force"] = F
+        np.savez_compressed(path, **rec)
+        print(name, "reference forces", F.tolist())
+
+
 def main():
     for name, geom, bas, opts in CASES:
         atoms = geom()
@@ -143,5 +160,7 @@ if __name__ == "__main__":
         add_oneint()
     elif "--iters" in sys.argv[1:]:
         add_scf_iters()
+    elif "--forces" in sys.argv[1:]:
+        add_forces()
     else:
         main()
