@@ -1,4 +1,5 @@
-"""Served stream of RHF/UHF SCF energy jobs on one device, with continuous batching.
+"""Served stream of RHF/UHF SCF energy and energy+gradient jobs on one device, with continuous
+batching.
 
 Requests arrive over time (e.g. Poisson arrivals, `poisson_requests`).  The server admits a
 request once it has arrived, a slot is free (at most `max_active` jobs in flight) and its
@@ -10,7 +11,8 @@ every active job (difference-density J/K build, Fock, cuSOLVER eigensolve, densi
 nothing read back), and only then reads each job's energy and density change: the steps of
 all jobs are in flight on the GPU at once, and a request that arrives meanwhile joins at the
 next round.  A job leaves when it meets the reference's convergence test (or its iteration
-cap) and frees its slot and memory.
+cap) -- after its nuclear gradient, when the request asks for one (scf.SCFJob.gradient, on the
+job's resident state) -- and frees its slot and memory.
 
 Each job runs exactly the single-job algorithm (scf.SCFJob), so its result is the one it gets
 alone, up to the order of floating-point atomics in the J/K build.
@@ -37,10 +39,12 @@ def footprint_bytes(atoms_angstrom, basis_name):
     return int(8 * 40 * n * n + pairs + (1 << 20))
 
 
-def poisson_requests(seed, count, rate, heavy=(2, 40), doublet_fraction=0.5, basis="631g_star"):
+def poisson_requests(seed, count, rate, heavy=(2, 40), doublet_fraction=0.5, basis="631g_star",
+                     gradient_fraction=0.5):
     """`count` requests with exponential inter-arrival times of mean 1/rate (seconds): seeded
     random organics (molecules.random_organic); a `doublet_fraction` of them become UHF
-    doublets by removing one hydrogen."""
+    doublets by removing one hydrogen; a `gradient_fraction` ask for the nuclear gradient as
+    well as the energy."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -50,8 +54,9 @@ def poisson_requests(seed, count, rate, heavy=(2, 40), doublet_fraction=0.5, bas
         uhf = bool(rng.random() < doublet_fraction)
         if uhf:
             atoms = M.remove_one_h(atoms, rng)
+        grad = bool(rng.random() < gradient_fraction)
         out.append({"id": i, "atoms": atoms, "basis": basis, "arrival": t, "charge": 0,
-                    "mult": 2 if uhf else 1})
+                    "mult": 2 if uhf else 1, "gradient": grad})
     return out
 
 
@@ -124,8 +129,9 @@ class Server:
                 r, job, fp, ta = entry
                 conv = job.update_finish()
                 if conv or job.iters >= self.max_iter:
+                    grad = job.gradient() if (r.get("gradient") and conv) else None
                     tf = clock()
-                    results[r["id"]] = {"id": r["id"], "energy": job.energy, "iters": job.iters,
+                    results[r["id"]] = {"id": r["id"], "energy": job.energy, "iters": job.iters, "gradient": grad,
                                         "converged": bool(conv), "nbf": job.n, "restricted": job.restricted,
                                         "arrival": r["arrival"] if realtime else 0.0, "admitted": ta,
                                         "finished": tf,
@@ -144,13 +150,15 @@ class Server:
 
 def solve_alone(request, device=0, scf_conv=1e-8, fp32_below=0.0):
     """The same job by itself (the plain one-at-a-time GPU path): (energy, iterations,
-    seconds of its SCF loop, set-up seconds)."""
+    seconds of its SCF loop and gradient, set-up seconds, gradient or None)."""
     t0 = time.perf_counter()
     job = SCFJob(request["atoms"], request["basis"], charge=request.get("charge", 0), mult=request.get("mult"),
                  scf_conv=scf_conv, device=device, fp32_below=fp32_below)
     t1 = time.perf_counter()
     e = job.run()
-    out = (e, job.iters, job.seconds, t1 - t0)
+    grad = job.gradient() if (request.get("gradient") and job.converged) else None
+    t2 = time.perf_counter()
+    out = (e, job.iters, t2 - t1, t1 - t0, grad)
     job.close()
     return out
 

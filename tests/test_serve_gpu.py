@@ -1,5 +1,6 @@
-"""Served stream on the GPU: jobs of different sizes and spins (RHF and UHF doublets) run
-concurrently with continuous batching; each job's served result must be the result it gets
+"""Served stream on the GPU: energy and energy+gradient jobs of different sizes and spins (RHF
+and UHF doublets) run concurrently with continuous batching; each job's served result (energy,
+and the gradient where asked) must be the result it gets
 alone (same SCF algorithm; only the order of FP64 atomics in the J/K builds differs), also when
 the HBM budget holds only a few jobs at a time.  Tolerance: 1e-9 Eh and the same number of SCF
 iterations (+-1)."""
@@ -23,8 +24,9 @@ def _requests(sqb):
     rng = np.random.default_rng(11)
     for k in (3, 4):
         m = sqb.molecules.random_organic(rng, k)
-        reqs.append({"atoms": m, "basis": "631g_star", "charge": 0, "mult": 1})
-        reqs.append({"atoms": sqb.molecules.remove_one_h(m, rng), "basis": "631g_star", "charge": 0, "mult": 2})
+        reqs.append({"atoms": m, "basis": "631g_star", "charge": 0, "mult": 1, "gradient": True})
+        reqs.append({"atoms": sqb.molecules.remove_one_h(m, rng), "basis": "631g_star", "charge": 0, "mult": 2,
+                     "gradient": True})
     for i, r in enumerate(reqs):
         r["id"] = i
         r["arrival"] = 0.05 * i
@@ -54,6 +56,8 @@ def test_served_results_equal_alone(two_slots_by_memory):
         assert o["converged"]
         assert abs(o["energy"] - a[0]) <= TOL, (r["id"], o["energy"], a[0])
         assert abs(o["iters"] - a[1]) <= 1
+        if r.get("gradient"):
+            assert np.abs(o["gradient"] - a[4]).max() <= 1e-8
     os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
     with open(os.path.join(ROOT, "gpurun_out", "serve_vs_alone_%d.json" % two_slots_by_memory), "w") as f:
         json.dump({"jobs": out, "stats": srv.stats}, f)
