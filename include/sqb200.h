@@ -110,22 +110,23 @@ const char *sqb200_jk_class_name(int k);
  * counterpart: the reference computes every quartet in FP64. */
 int sqb200_jk_set_precision(sqb200_jk *ctx, double fp32_below);
 
-/* Tile autotuner.  Classes whose ket functions the kernels split into passes have two FP64
- * forms: the narrow tile (more passes, fewer registers) and the wide tile (fewer passes; each
- * pass re-derives the Boys function and R for more ket functions).  This call runs the build's
- * prologue for the given density and cutoffs (as sqb200_jk_build_device) and times both forms
- * of every such class on the build's own work list (CUDA events, 2 launches each after one
- * untimed), then keeps the faster form per class for the context's following builds.  Leaves
- * the context's accumulators dirty (the next build clears them); synchronous.  No reference
- * counterpart. */
+/* Tile autotuner.  Every class has up to three FP64 forms: 0 the narrow tile (ket functions
+ * split into passes of at most 64 accumulator doubles), 1 the wide tile (fewer, larger passes;
+ * classes with several passes only), 2 the swapped loop roles (outer loop over the thread's own
+ * ket primitives, inner loop over the CTA's bra primitives in shared memory; passes split the
+ * bra functions).  This call runs the build's prologue for the given density and cutoffs (as
+ * sqb200_jk_build_device), times every form of every class on the build's own work list (CUDA
+ * events, 2 launches each after one untimed) and keeps the fastest per class for the context's
+ * following builds.  Leaves the context's accumulators dirty (the next build clears them);
+ * synchronous.  No reference counterpart. */
 int sqb200_jk_autotune(sqb200_jk *ctx, const double *dPA, const double *dPB, int restricted,
                        double scf_cutoff, double fixed_cutoff, double dscreen_rmax, void *stream);
 
-/* Read (sqb200_jk_tiles) or set (sqb200_jk_set_tiles) the per-class tile choice: wide[k] = 1
- * wide tile, 0 narrow tile, -1 (read only) class k has one form.  sqb200_jk_tiles returns the
- * number of entries written (at most n). */
-int sqb200_jk_tiles(sqb200_jk *ctx, int *wide, int n);
-int sqb200_jk_set_tiles(sqb200_jk *ctx, const int *wide, int n);
+/* Read (sqb200_jk_tiles) or set (sqb200_jk_set_tiles) the per-class FP64 form: 0, 1 or 2 as
+ * above; -1 (read only) class k has one form.  Setting a form a class lacks selects 0.
+ * sqb200_jk_tiles returns the number of entries written (at most n). */
+int sqb200_jk_tiles(sqb200_jk *ctx, int *form, int n);
+int sqb200_jk_set_tiles(sqb200_jk *ctx, const int *form, int n);
 
 /* One-electron integrals of the context's basis on its device: overlap S, kinetic T and
  * nuclear attraction V = -sum_C Z_C <p|1/|r-C||q> for natom point charges Z at axyz (bohr),

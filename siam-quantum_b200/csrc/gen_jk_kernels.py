@@ -57,6 +57,10 @@ STATE_MAX_WIDE = int(os.environ.get("SQB_STATE_MAX_WIDE", "128"))
 # thread, thread-fastest): only the Hermite intermediates G (at most G_MAX doubles) stay in
 # registers, so a pass can hold more ket functions without spilling
 WIDE_SMEM = int(os.environ.get("SQB_WIDE_SMEM", "0"))
+# the swapped-role form (outer loop over the thread's ket primitives, inner over the shared bra
+# primitives in shared memory): emitted for every class, state budget of its passes
+SWAP = int(os.environ.get("SQB_SWAP", "1"))
+STATE_MAX_SWAP = int(os.environ.get("SQB_STATE_MAX_SWAP", "128"))
 G_MAX = int(os.environ.get("SQB_G_MAX", "48"))
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
 F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
@@ -415,9 +419,188 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
     return "\n".join(out) + "\n", meta
 
 
-def emit_digest(em, spin, blk, nab, na, nb_, nd):
-    """Digest the contracted block o<ab>_<cd> (cd in blk) into the J/K accumulators.
-    Expects PA, PB (unrestricted), PT, N, bp, kp, deg and jab<ab> in scope; returns flops."""
+def swap_worthwhile(bra, ket):
+    """The swapped form is emitted where a pass can hold at least two bra functions (or the only
+    one) and the class needs at most 8 passes (beyond that the code size grows past what ptxas
+    compiles in reasonable time, and the form repeats the Boys function and R too often to pay)."""
+    fb, _, _ = etable(bra)
+    fk, _, _ = etable(ket)
+    Hk = {h for f in fk for h in nz(f)}
+    per = min(len(fb), STATE_MAX_SWAP // (len(Hk) + len(fk)))
+    return per >= min(2, len(fb)) and (len(fb) + per - 1) // per <= 8
+
+
+def gen_class_swap(bra, ket, spin, state_max):
+    """The class kernel with the loop roles swapped (suffix _s): the outer loop runs over the
+    primitives of the thread's own ket pair (each record read from global memory once per pass),
+    the inner loop over the CTA-shared bra pair's primitives in shared memory (broadcast reads).
+    The inner loop contracts the bra E tables, G[ab][k] = sum_i sum_h Eb_i[ab][h] R_{h+k}; after
+    it, the ket E tables flush, out[ab][cd] += sum_k (-1)^|k| Ek_j[cd][k] G[ab][k].  Passes
+    (grid.y) split the bra functions: G + out of one pass <= state_max doubles.  FP64 only."""
+    fb, offb, layb = etable(bra)
+    fk, offk, layk = etable(ket)
+    nab, ncd = len(fb), len(fk)
+    Hk = sorted({h for f in fk for h in nz(f)}, key=lambda x: (sum(x), x))
+    kidx = {h: i for i, h in enumerate(Hk)}
+    na, nb_ = len(COMP[bra[0]]), len(COMP[bra[1]])
+    nc, nd = len(COMP[ket[0]]), len(COMP[ket[1]])
+    NB = 5 + len(layb)
+    NK = 5 + len(layk)
+    per = max(1, min(nab, state_max // (len(Hk) + ncd)))
+    blocks = [list(range(s0, min(nab, s0 + per))) for s0 in range(0, nab, per)]
+    name = "jk_%s_%s_%s_s" % (bra, ket, spin)
+    Hb_all = sorted({h for f in fb for h in nz(f)}, key=lambda x: (sum(x), x))
+    fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks),
+          "alg_prim": alg_prim_flops(fk, Hb_all, "double", "fma"), "o_dbl": 0}
+    em = Emitter()
+    out = ['extern "C" __global__ void __launch_bounds__(%d)' % CTA,
+           "%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name]
+    em("extern __shared__ double sbra[];")
+    em("const sqb::WorkItem it = items[blockIdx.x];")
+    em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
+    em("const sqb::MolRec mr = a.mols[it.mol];        // the molecule of this work item")
+    em("double* __restrict__ Jacc = a.Jacc + mr.moff;")
+    em("double* __restrict__ KAacc = a.KAacc + mr.moff;")
+    em("double* __restrict__ KBacc = a.KBacc + mr.moff;")
+    em("const int N = mr.nbf;")
+    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
+    em("__syncthreads();")
+    em("const int isplit = it.isplit;                 // threads sharing one quartet (ket primitives split)")
+    em("const int kl = threadIdx.x / isplit, grp = threadIdx.x - kl * isplit;")
+    em("const int pass = blockIdx.y;                   // block of bra functions handled by this CTA")
+    em("bool ok = kl < it.cnt;")
+    em("sqb::PairRec kp = bp;")
+    em("double deg = 0.0;")
+    em("if (ok) {")
+    em.ind += 1
+    em("kp = a.ket_pairs[it.k0 + kl];")
+    em("const double r = bp.schwarz * kp.schwarz;")
+    em("ok = !(r < mr.cut_outer) && !(r < mr.cut_fixed);")
+    em("if (ok && r < mr.dscreen_rmax) {")
+    em("  const bool bf = (bp.P > kp.P) || (bp.P == kp.P && bp.Q >= kp.Q);")
+    em("  const int P = bf ? bp.P : kp.P, Q = bf ? bp.Q : kp.Q, I = bf ? kp.P : bp.P, J = bf ? kp.Q : bp.Q;")
+    em("  const double* PM = a.PM + mr.pmoff; const int ns = mr.ns;")
+    em("  const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];")
+    em("  ok = !(r * mp < mr.cut_fixed);")
+    em("}")
+    em("deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + kl) ? 0.5 : 1.0);")
+    em.ind -= 1
+    em("}")
+    for ab in range(nab):
+        em("double jab%d = 0.0;" % ab)
+    em("unsigned long long nprimq = 0, nflush = 0;")
+    em("if (ok) {")
+    em.ind += 1
+    em("const double* __restrict__ kprim = a.ket_prims + kp.poff;")
+    em("const int nbp = bp.nprim, nkp = kp.nprim;")
+    em("nflush = pass == 0 ? (unsigned long long)((nkp - grp + isplit - 1) / isplit) : 0ull;")
+    em("const double* __restrict__ PA = a.PA + mr.moff;")
+    if spin == "U":
+        em("const double* __restrict__ PB = a.PB + mr.moff;")
+    em("const double* __restrict__ PT = a.PT + mr.moff;")
+    em("switch (pass) {")
+    for bi, blk in enumerate(blocks):
+        em("case %d: {  // bra functions %s" % (bi, blk))
+        em.ind += 1
+        for ab in blk:
+            for cd in range(ncd):
+                em("double o%d_%d = 0;" % (ab, cd))
+        em("for (int j = grp; j < nkp; j += isplit) {")
+        em.ind += 1
+        em("const double* __restrict__ kj = kprim + j * %d;" % NK)
+        em("const double q = kj[0], Qx = kj[1], Qy = kj[2], Qz = kj[3], kq = kj[4];")
+        for ab in blk:
+            for k in Hk:
+                em("double g%d_%d = 0;" % (ab, kidx[k]))
+        # bra E-table entries this block reads (from shared memory, inside the inner loop)
+        bent = []
+        for ab in blk:
+            for e, h in enumerate(nz(fb[ab])):
+                bent.append((ab, e, h))
+        em("for (int i = 0; i < nbp; ++i) {")
+        em.ind += 1
+        em("const double* __restrict__ bi = sbra + i * %d;" % NB)
+        em("const double p = bi[0];")
+        em("const double pq = p + q;")
+        em("const double rs = rsqrt(pq);")
+        em("if (TWO_PI_2_5 * bi[4] * kq * rs < PRIM_CUTOFF) continue;")
+        if bi == 0:
+            em("++nprimq;")
+        em("const double alpha = p * q * (rs * rs);")
+        em("const double X = bi[1] - Qx, Y = bi[2] - Qy, Z = bi[3] - Qz;")
+        em("const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));")
+        need = set()
+        cons = {}
+        for (ab, e, h) in bent:
+            for k in Hk:
+                key = (h[0] + k[0], h[1] + k[1], h[2] + k[2])
+                need.add(key)
+                cons.setdefault(key, []).append((ab, e, k))
+        Lp = max(sum(x) for x in need)
+        em("double F[%d];" % (Lp + 1))
+        em("sqb::boys<%d>(T, a.boys_tab, F);" % Lp)
+        em("const double s0 = TWO_PI_2_5 * rs;")
+        em("const double m2a = -2.0 * alpha;")
+        em("double w = s0;")
+        pf = 9 + 2 + 3 + 5 + boys_flops(Lp) + 2
+        for n in range(Lp + 1):
+            if n > 0:
+                em("w *= m2a;")
+                pf += 1
+            em("const double b%d = w * F[%d];" % (n, n))
+            pf += 1
+        for (ab, e, h) in bent:
+            em("const double eb%d_%d = bi[%d];" % (ab, e, 5 + offb[ab] + e))
+        rn, rf = gen_R(em, Lp, need, cons=cons, emit_use=lambda key, nm: [
+            em("g%d_%d = fma(eb%d_%d, %s, g%d_%d);" % (ab, kidx[k], ab, e, nm, ab, kidx[k]))
+            for (ab, e, k) in cons.get(key, [])], rt="double", fma="fma")
+        pf += rf + 2 * sum(len(v) for v in cons.values())
+        em.ind -= 1
+        em("}")
+        # flush with the ket E tables (signed by (-1)^(tau+nu+phi))
+        ff = 0
+        for cd in range(ncd):
+            for e, k in enumerate(nz(fk[cd])):
+                sg = "-" if sum(k) % 2 else ""
+                em("{ const double ek = %skj[%d];" % (sg, 5 + offk[cd] + e))
+                for ab in blk:
+                    em("  o%d_%d = fma(ek, g%d_%d, o%d_%d);" % (ab, cd, ab, kidx[k], ab, cd))
+                    ff += 2
+                em("}")
+        em.ind -= 1
+        em("}")
+        fl["prim"] += pf
+        fl["flush"] += ff
+        qf = emit_digest(em, spin, list(range(ncd)), nab, na, nb_, nd, ablk=blk)
+        fl["quartet"] += qf
+        em.ind -= 1
+        em("} break;")
+    em("}")
+    em.ind -= 1
+    em("}")
+    em("{")
+    em("  const int fP = bp.fP, fQ = bp.fQ;")
+    em("  const double s2 = 2.0 * deg;")
+    for ab in range(nab):
+        aa, bb = divmod(ab, nb_)
+        em("  { const double v = sqb::warp_sum(s2 * jab%d); if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(Jacc + (fP + %d) * N + fQ + %d, v); }" % (ab, aa, bb))
+    em("}")
+    em("sqb::count_add(a.counters + 0, (ok && grp == 0 && pass == 0) ? 1ull : 0ull);")
+    em("sqb::count_add(a.counters + 1, nprimq);")
+    em("sqb::count_add(a.counters + 2, nflush);")
+    em("sqb::count_add(a.counters + 3, (ok && pass == 0) ? 1ull : 0ull);")
+    out.extend(em.lines)
+    out.append("}")
+    meta = {"name": name, "bra": bra, "ket": ket, "spin": spin, "nab": nab, "ncd": ncd,
+            "neb": len(layb), "nek": len(layk), "Lt": pair_L(bra) + pair_L(ket), "flops": fl}
+    return "\n".join(out) + "\n", meta
+
+
+def emit_digest(em, spin, blk, nab, na, nb_, nd, ablk=None):
+    """Digest the contracted block o<ab>_<cd> (cd in blk, ab in ablk -- all bra functions by
+    default) into the J/K accumulators.  Expects PA, PB (unrestricted), PT, N, bp, kp, deg and
+    jab<ab> in scope; returns flops."""
+    abs_ = list(range(nab)) if ablk is None else list(ablk)
     qf = 0
     cset = sorted({cd // nd for cd in blk})
     dset = sorted({cd % nd for cd in blk})
@@ -427,7 +610,7 @@ def emit_digest(em, spin, blk, nab, na, nb_, nd):
     for cd in blk:
         c, d = divmod(cd, nd)
         em("const double ptk%d = PT[(fI + %d) * N + fJ + %d];" % (cd, c, d))
-    for ab in range(nab):
+    for ab in abs_:
         aa, bb = divmod(ab, nb_)
         em("const double ptb%d = PT[(fP + %d) * N + fQ + %d];" % (ab, aa, bb))
     spins = [("A", "PA")] + ([("B", "PB")] if spin == "U" else [])
@@ -435,7 +618,7 @@ def emit_digest(em, spin, blk, nab, na, nb_, nd):
         for bb in range(nb_):
             for d in dset:
                 em("const double %sbd%d_%d = %s[(fQ + %d) * N + fJ + %d];" % (s, bb, d, P_, bb, d))
-        for aa in range(na):
+        for aa in sorted({ab // nb_ for ab in abs_}):
             for d in dset:
                 em("const double %sad%d_%d = %s[(fP + %d) * N + fJ + %d];" % (s, aa, d, P_, aa, d))
         for bb in range(nb_):
@@ -444,19 +627,19 @@ def emit_digest(em, spin, blk, nab, na, nb_, nd):
         for aa in range(na):
             for c in cset:
                 em("const double %sac%d_%d = %s[(fP + %d) * N + fI + %d];" % (s, aa, c, P_, aa, c))
-    for ab in range(nab):
+    for ab in abs_:
         terms = " + ".join("o%d_%d * ptk%d" % (ab, cd, cd) for cd in blk)
         em("jab%d += %s;" % (ab, terms))
         qf += 2 * len(blk)
     for cd in blk:
         c, d = divmod(cd, nd)
-        terms = " + ".join("o%d_%d * ptb%d" % (ab, cd, ab) for ab in range(nab))
+        terms = " + ".join("o%d_%d * ptb%d" % (ab, cd, ab) for ab in abs_)
         em("atomicAdd(Jacc + (fI + %d) * N + fJ + %d, 2.0 * deg * (%s));" % (c, d, terms))
-        qf += 2 * nab + 2
+        qf += 2 * len(abs_) + 2
     for s, _ in spins:
         acc = "KAacc" if s == "A" else "KBacc"
         tg = {}
-        for ab in range(nab):
+        for ab in abs_:
             aa, bb = divmod(ab, nb_)
             for cd in blk:
                 c, d = divmod(cd, nd)
@@ -737,6 +920,11 @@ def main():
                 s4, m4 = gen_class(bra, ket, spin, "D", STATE_MAX_WIDE, "_w")
                 src.append(s4)
                 m["wide"] = m4
+            m["swap"] = None
+            if SWAP and swap_worthwhile(bra, ket):
+                s5, m5 = gen_class_swap(bra, ket, spin, STATE_MAX_SWAP)
+                src.append(s5)
+                m["swap"] = m5
             m["f32"] = None
             if pair_L(bra) + pair_L(ket) <= F32_MAX_L:
                 s3, m3 = gen_class(bra, ket, spin, "F")
@@ -757,6 +945,8 @@ def main():
             reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["f32"]["name"])
         if m["wide"]:
             reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["wide"]["name"])
+        if m["swap"]:
+            reg.append('extern "C" __global__ void %s(const sqb::JKArgs, const sqb::WorkItem*);' % m["swap"]["name"])
     reg.append("")
     reg.append("namespace sqb {")
     reg.append("const char* const kPairClassNames[%d] = {%s};" % (len(PAIRS), ", ".join('"%s"' % p for p in PAIRS)))
@@ -784,11 +974,18 @@ def main():
         reg.append('   %d,' % r["flops"]["alg_prim"])
         wr, wu = r["wide"], u["wide"]
         if wr:
-            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d, %d},' % (
+            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d, %d,' % (
                 wr["flops"]["passes"], wr["name"], wu["name"], wr["flops"]["prim"], wr["flops"]["flush"],
                 wr["flops"]["quartet"], wr["flops"]["o_dbl"]))
         else:
-            reg.append('   0, nullptr, nullptr, 0, 0, 0, 0},')
+            reg.append('   0, nullptr, nullptr, 0, 0, 0, 0,')
+        sr, su = r["swap"], u["swap"]
+        if sr:
+            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+                sr["flops"]["passes"], sr["name"], su["name"], sr["flops"]["prim"], sr["flops"]["flush"],
+                sr["flops"]["quartet"]))
+        else:
+            reg.append('   0, nullptr, nullptr, 0, 0, 0},')
     reg.append("};")
     reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
     reg.append("}  // namespace sqb")
@@ -798,6 +995,7 @@ def main():
     fj.update({m["ws"]["name"]: m["ws"]["flops"] for m in metas if m["ws"]})
     fj.update({m["f32"]["name"]: m["f32"]["flops"] for m in metas if m["f32"]})
     fj.update({m["wide"]["name"]: m["wide"]["flops"] for m in metas if m["wide"]})
+    fj.update({m["swap"]["name"]: m["swap"]["flops"] for m in metas if m["swap"]})
     write_if_changed(os.path.join(outdir, "jk_flops.json"), json.dumps(fj, indent=0))
     write_if_changed(os.path.join(outdir, "files.txt"), "\n".join(files) + "\n")
     print("generated %d kernels in %d files" % (len(metas), len(files)))

@@ -219,7 +219,8 @@ struct sqb200_jk {
   double fp32_below = 0.0;      // quartets with Schwarz product below this use the FP32 form
   bool use_ws = true;           // warp-specialised form where a class has one (SQB200_WS=0 disables)
   std::vector<char> ran_ws;     // per class kernel: which form the last build launched
-  std::vector<char> wide;       // per class kernel: run the wide-tile FP64 form (sqb200_jk_autotune)
+  std::vector<char> form;       // per class kernel: FP64 form to run, 0 narrow / 1 wide / 2 swapped (autotuner)
+  std::vector<char> ran_form;   // per class kernel: the FP64 form the last build launched
   std::vector<long long> last_counts;
   long long last_flops = 0;
   int last_launches = 0;        // kernels enqueued by the last build
@@ -744,20 +745,25 @@ struct SegLaunch {
   const sqb::WorkItem* items = nullptr;
 };
 
-// The form of class kernel v (v >= K: FP32 form) for spin uhf; wide selects the wide-tile FP64
-// form where the class has one.
-// Returns true when the wide form was picked.
-bool pick_form(const sqb::ClassKernel& K, bool f32, int uhf, bool wide, const void** fn, int* passes) {
-  if (f32) { *fn = uhf ? K.fn_u32 : K.fn_r32; *passes = K.passes32; return false; }
-  if (wide && K.fn_rw) { *fn = uhf ? K.fn_uw : K.fn_rw; *passes = K.passes_w; return true; }
+// FP64 forms of a class: 0 narrow tile, 1 wide tile, 2 swapped loop roles.
+bool has_form(const sqb::ClassKernel& K, int form) {
+  return form == 0 || (form == 1 && K.fn_rw) || (form == 2 && K.fn_rs);
+}
+
+// The kernel of class K (FP32 form when f32) for spin uhf in FP64 form `form` (falls back to the
+// narrow tile where the class lacks it).  Returns the FP64 form picked (0 for the FP32 form).
+int pick_form(const sqb::ClassKernel& K, bool f32, int uhf, int form, const void** fn, int* passes) {
+  if (f32) { *fn = uhf ? K.fn_u32 : K.fn_r32; *passes = K.passes32; return 0; }
+  if (form == 1 && K.fn_rw) { *fn = uhf ? K.fn_uw : K.fn_rw; *passes = K.passes_w; return 1; }
+  if (form == 2 && K.fn_rs) { *fn = uhf ? K.fn_us : K.fn_rs; *passes = K.passes_s; return 2; }
   *fn = uhf ? K.fn_u : K.fn_r;
   *passes = K.passes;
-  return false;
+  return 0;
 }
 
 // Shared-memory accumulators of the wide form: the region follows the staged bra primitives.
-void add_acc_region(const sqb::ClassKernel& K, bool wide_used, SegLaunch& L) {
-  if (!wide_used || K.w_o_dbl <= 0) return;
+void add_acc_region(const sqb::ClassKernel& K, int form_used, SegLaunch& L) {
+  if (form_used != 1 || K.w_o_dbl <= 0) return;
   const size_t off = (L.smem + 15) / 16 * 16;
   L.a.so_off = (int)(off / sizeof(double));
   L.smem = off + (size_t)K.w_o_dbl * L.block.x * sizeof(double);
@@ -789,9 +795,9 @@ int enqueue(const SegLaunch& L, cudaStream_t st) {
   return SQB200_OK;
 }
 
-// Segment s of a single-context work list; wide < 0 takes the context's tile choice.
+// Segment s of a single-context work list; form < 0 takes the context's choice.
 SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const double* dPA, const double* dPB,
-                     int uhf, int wide) {
+                     int uhf, int form) {
   SegLaunch L;
   const int v = w->kernel[s];
   const bool f32 = v >= sqb::kNumClassKernels;
@@ -819,9 +825,10 @@ SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const dou
   if (ws) {
     L.fn = uhf ? K.ws_u : K.ws_r;
   } else {
-    const bool wu = pick_form(K, f32, uhf, wide < 0 ? (c->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
+    const int fu = pick_form(K, f32, uhf, form < 0 ? c->form[kidx] : form, &L.fn, &passes);
+    if (!f32) c->ran_form[kidx] = (char)fu;
     L.block = dim3(128);
-    add_acc_region(K, wu, L);
+    add_acc_region(K, fu, L);
   }
   L.grid = dim3(w->count[s], passes);
   L.block = dim3(ws ? 32 * K.ws_warps : 128);
@@ -890,15 +897,19 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
 // from its four counters [quartets, primitive quartets, bra flushes, digestions]: per
 // primitive quartet the pass-free count (Boys function and R once), per flush and digestion
 // the operations of the form that ran (those are not repeated across passes).
-double kernel_flops(const sqb200_jk* c, int v, const unsigned long long* h) {
+double kernel_flops_form(int v, int form, const unsigned long long* h) {
   const int K_ = sqb::kNumClassKernels;
   const bool f32 = v >= K_;
   const sqb::ClassKernel& K = sqb::kClassKernels[f32 ? v - K_ : v];
-  const bool ws = !f32 && v < (int)c->ran_ws.size() && c->ran_ws[v];
   const double fp = K.alg_flops_prim;
-  const double ff = f32 ? K.f32_flops_flush : ws ? K.ws_flops_flush : K.flops_flush;
-  const double fq = f32 ? K.f32_flops_quartet : ws ? K.ws_flops_quartet : K.flops_quartet;
+  const double ff = f32 ? K.f32_flops_flush : form == 1 ? K.w_flops_flush : form == 2 ? K.s_flops_flush : K.flops_flush;
+  const double fq = f32 ? K.f32_flops_quartet : form == 1 ? K.w_flops_quartet : form == 2 ? K.s_flops_quartet : K.flops_quartet;
   return (double)h[1] * fp + (double)h[2] * ff + (double)h[3] * fq;
+}
+
+double kernel_flops(const sqb200_jk* c, int v, const unsigned long long* h) {
+  const bool f32 = v >= sqb::kNumClassKernels;
+  return kernel_flops_form(v, f32 || v >= (int)c->ran_form.size() ? 0 : c->ran_form[v], h);
 }
 
 // Mean device time (ms) of `reps` launches of L on st after one untimed launch.
@@ -940,7 +951,8 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   const char* ws_env = getenv("SQB200_WS");
   c->use_ws = !(ws_env && ws_env[0] == '0');
   c->ran_ws.assign(sqb::kNumClassKernels, 0);
-  c->wide.assign(sqb::kNumClassKernels, 0);
+  c->form.assign(sqb::kNumClassKernels, 0);
+  c->ran_form.assign(sqb::kNumClassKernels, 0);
   c->nbf = nbf;
   int rc = build_shells(nbf, nprim, lmn, xyz, exps, ncoefs, c->shells);
   if (rc) { delete c; return rc; }
@@ -1027,26 +1039,35 @@ int sqb200_jk_autotune(sqb200_jk* c, const double* dPA, const double* dPB, int r
   k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM);
   for (size_t s = 0; s < w->kernel.size(); ++s) {
     const int v = w->kernel[s];
-    if (v >= sqb::kNumClassKernels || !sqb::kClassKernels[v].fn_rw) continue;
-    double tn = 0.0, tw = 0.0;
-    rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, 0), st, 2, &tn);
-    if (!rc) rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, 1), st, 2, &tw);
-    if (rc) return rc;
-    c->wide[v] = tw < tn ? 1 : 0;
+    if (v >= sqb::kNumClassKernels) continue;
+    double best = 0.0;
+    int bf = 0;
+    for (int f = 0; f < 3; ++f) {
+      if (!has_form(sqb::kClassKernels[v], f)) continue;
+      double t = 0.0;
+      rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, f), st, 2, &t);
+      if (rc) return rc;
+      if (f == 0 || t < best) { best = t; bf = f; }
+    }
+    c->form[v] = (char)bf;
   }
   CUDA_OK(cudaStreamSynchronize(st));
   return SQB200_OK;
 }
 
-int sqb200_jk_tiles(sqb200_jk* c, int* wide, int n) {
-  if (!c || !wide) return fail(SQB200_EINVAL, "null argument");
-  for (int k = 0; k < n && k < sqb::kNumClassKernels; ++k) wide[k] = sqb::kClassKernels[k].fn_rw ? c->wide[k] : -1;
+int sqb200_jk_tiles(sqb200_jk* c, int* form, int n) {
+  if (!c || !form) return fail(SQB200_EINVAL, "null argument");
+  for (int k = 0; k < n && k < sqb::kNumClassKernels; ++k) {
+    const sqb::ClassKernel& K = sqb::kClassKernels[k];
+    form[k] = (K.fn_rw || K.fn_rs) ? c->form[k] : -1;
+  }
   return std::min(n, sqb::kNumClassKernels);
 }
 
-int sqb200_jk_set_tiles(sqb200_jk* c, const int* wide, int n) {
-  if (!c || !wide) return fail(SQB200_EINVAL, "null argument");
-  for (int k = 0; k < n && k < sqb::kNumClassKernels; ++k) c->wide[k] = wide[k] > 0 ? 1 : 0;
+int sqb200_jk_set_tiles(sqb200_jk* c, const int* form, int n) {
+  if (!c || !form) return fail(SQB200_EINVAL, "null argument");
+  for (int k = 0; k < n && k < sqb::kNumClassKernels; ++k)
+    c->form[k] = (char)(has_form(sqb::kClassKernels[k], form[k]) ? form[k] : 0);
   return SQB200_OK;
 }
 
@@ -1445,7 +1466,7 @@ struct sqb200_batch {
   size_t items_cap = 0;
   bool have_step = false;
   std::vector<unsigned long long> last_counts;
-  std::vector<char> wide;               // per class kernel: wide-tile FP64 form (sqb200_batch_autotune)
+  std::vector<char> form;               // per class kernel: FP64 form (sqb200_batch_autotune)
   int last_launches = 0;
   int nside = -1;
   std::vector<cudaStream_t> side;
@@ -1586,7 +1607,7 @@ extern "C" int sqb200_batch_create(sqb200_batch** out, int nmol, sqb200_jk* cons
   if (e == cudaSuccess) e = cudaMemcpy(b->d_shn, nf.data(), nf.size() * sizeof(int), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(SQB200_ECUDA, cudaGetErrorString(e));
-  b->wide.assign(sqb::kNumClassKernels, 0);
+  b->form.assign(sqb::kNumClassKernels, 0);
   b->rec.resize(nmol);
   for (int m = 0; m < nmol; ++m)
     b->rec[m] = sqb::MolRec{b->moff[m], b->pmoff[m], mols[m]->nbf, mols[m]->ns, 0.0, 0.0, 0.0, b->shoff[m], 0};
@@ -1666,8 +1687,8 @@ extern "C" int sqb200_batch_set_step(sqb200_batch* b, const int* restricted, con
   return SQB200_OK;
 }
 
-// Segment s of a batch's work list; wide < 0 takes the batch's tile choice.
-SegLaunch seg_batch(sqb200_batch* b, size_t s, const double* dPA, const double* dPB, int wide) {
+// Segment s of a batch's work list; form < 0 takes the batch's choice.
+SegLaunch seg_batch(sqb200_batch* b, size_t s, const double* dPA, const double* dPB, int form) {
   SegLaunch L;
   const int K_ = sqb::kNumClassKernels;
   const int v = b->kernel[s], uhf = b->spin[s];
@@ -1690,10 +1711,10 @@ SegLaunch seg_batch(sqb200_batch* b, size_t s, const double* dPA, const double* 
   L.items = b->d_items + b->first[s];
   L.smem = (size_t)B.max_nprim * B.stride * (f32 ? sizeof(float) : sizeof(double));
   int passes = 1;
-  const bool wu = pick_form(K, f32, uhf, wide < 0 ? (b->wide[kidx] != 0) : wide != 0, &L.fn, &passes);
+  const int fu = pick_form(K, f32, uhf, form < 0 ? b->form[kidx] : form, &L.fn, &passes);
   L.grid = dim3(b->count[s], passes);
   L.block = dim3(128);
-  add_acc_region(K, wu, L);
+  add_acc_region(K, fu, L);
   return L;
 }
 
@@ -1712,18 +1733,24 @@ extern "C" int sqb200_batch_autotune(sqb200_batch* b, const double* dPA, const d
   cudaStream_t st = stream ? (cudaStream_t)stream : b->stream;
   batch_prologue(b, dPA, dPB, st);
   // a class with restricted and unrestricted segments keeps one choice: the summed time decides
-  std::vector<double> tn(sqb::kNumClassKernels, 0.0), tw(sqb::kNumClassKernels, 0.0);
+  std::vector<double> tf(3 * sqb::kNumClassKernels, 0.0);
   for (size_t s = 0; s < b->kernel.size(); ++s) {
     const int v = b->kernel[s];
-    if (v >= sqb::kNumClassKernels || !sqb::kClassKernels[v].fn_rw) continue;
-    double a = 0.0, w = 0.0;
-    int rc = time_seg(seg_batch(b, s, dPA, dPB, 0), st, 2, &a);
-    if (!rc) rc = time_seg(seg_batch(b, s, dPA, dPB, 1), st, 2, &w);
-    if (rc) return rc;
-    tn[v] += a;
-    tw[v] += w;
+    if (v >= sqb::kNumClassKernels) continue;
+    for (int f = 0; f < 3; ++f) {
+      if (!has_form(sqb::kClassKernels[v], f)) continue;
+      double t = 0.0;
+      const int rc = time_seg(seg_batch(b, s, dPA, dPB, f), st, 2, &t);
+      if (rc) return rc;
+      tf[3 * v + f] += t;
+    }
   }
-  for (int k = 0; k < sqb::kNumClassKernels; ++k) b->wide[k] = (tw[k] > 0.0 && tw[k] < tn[k]) ? 1 : 0;
+  for (int k = 0; k < sqb::kNumClassKernels; ++k) {
+    int bf = 0;
+    for (int f = 1; f < 3; ++f)
+      if (has_form(sqb::kClassKernels[k], f) && tf[3 * k + f] < tf[3 * k + bf]) bf = f;
+    b->form[k] = (char)bf;
+  }
   CUDA_OK(cudaStreamSynchronize(st));
   return SQB200_OK;
 }
@@ -1791,7 +1818,7 @@ extern "C" int sqb200_batch_stats(sqb200_batch* b, long long* out, int n) {
       const unsigned long long* c = &h[4 * (sp * 2 * K_ + v)];
       q += (long long)c[0];
       pq += (long long)c[1];
-      fl += kernel_flops(b->mols[0], v, c);
+      fl += kernel_flops_form(v, v < K_ ? b->form[v] : 0, c);
     }
   long long pairs = 0, shells = 0;
   for (const sqb200_jk* c : b->mols) {

@@ -40,6 +40,13 @@ struct ClassKernel {
   const void* fn_uw;
   int w_flops_prim, w_flops_flush, w_flops_quartet;
   int w_o_dbl;            // doubles per thread of the wide form's shared-memory accumulators (0: registers)
+  // swapped-role FP64 form: outer loop over the thread's ket primitives (global, once per
+  // pass), inner loop over the shared bra primitives (shared memory); passes split the bra
+  // functions; its flush counter counts ket primitives
+  int passes_s;
+  const void* fn_rs;
+  const void* fn_us;
+  int s_flops_prim, s_flops_flush, s_flops_quartet;
 };
 
 extern const ClassKernel kClassKernels[];

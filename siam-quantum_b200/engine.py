@@ -165,15 +165,16 @@ class JKEngine:
 
     def autotune(self, dPA, dPB=None, restricted=True, scf_cutoff=1e-10, fixed_cutoff=None,
                  dscreen_rmax=float("inf"), stream=None):
-        """Time the narrow and wide tile forms of every multi-pass class on this density's work
-        list and keep the faster per class (device pointers; synchronous)."""
+        """Time every FP64 form of every class (narrow tile, wide tile, swapped loop roles) on
+        this density's work list and keep the fastest per class (device pointers; synchronous)."""
         if fixed_cutoff is None:
             fixed_cutoff = scf_cutoff
         _check(_lib.sqb200_jk_autotune(self._ctx, dPA, dPA if dPB is None else dPB, int(bool(restricted)),
                                        scf_cutoff, fixed_cutoff, dscreen_rmax, stream))
 
     def tiles(self):
-        """Per class kernel: 1 wide tile, 0 narrow tile, -1 single form."""
+        """Per class kernel: the FP64 form, 0 narrow tile, 1 wide tile, 2 swapped loop roles
+        (-1: the class has one form)."""
         out = np.zeros(256, np.int32)
         n = _lib.sqb200_jk_tiles(self._ctx, out, len(out))
         if n < 0:
