@@ -61,6 +61,10 @@ WIDE_SMEM = int(os.environ.get("SQB_WIDE_SMEM", "0"))
 # primitives in shared memory): emitted for every class, state budget of its passes
 SWAP = int(os.environ.get("SQB_SWAP", "1"))
 STATE_MAX_SWAP = int(os.environ.get("SQB_STATE_MAX_SWAP", "128"))
+# swapped form with its contracted block in shared memory (slots per thread, touched once per
+# ket primitive at the flush): only G and the recursion stay in registers
+SWAP_SMEM_O = int(os.environ.get("SQB_SWAP_SMEM", "0"))
+G_MAX_SWAP = int(os.environ.get("SQB_G_MAX_SWAP", "40"))   # G doubles per pass of that form
 G_MAX = int(os.environ.get("SQB_G_MAX", "48"))
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
 F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
@@ -446,16 +450,19 @@ def gen_class_swap(bra, ket, spin, state_max):
     nc, nd = len(COMP[ket[0]]), len(COMP[ket[1]])
     NB = 5 + len(layb)
     NK = 5 + len(layk)
-    per = max(1, min(nab, state_max // (len(Hk) + ncd)))
+    SO = SWAP_SMEM_O
+    per = max(1, min(nab, (G_MAX_SWAP // len(Hk)) if SO else state_max // (len(Hk) + ncd)))
     blocks = [list(range(s0, min(nab, s0 + per))) for s0 in range(0, nab, per)]
     name = "jk_%s_%s_%s_s" % (bra, ket, spin)
     Hb_all = sorted({h for f in fb for h in nz(f)}, key=lambda x: (sum(x), x))
     fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks),
-          "alg_prim": alg_prim_flops(fk, Hb_all, "double", "fma"), "o_dbl": 0}
+          "alg_prim": alg_prim_flops(fk, Hb_all, "double", "fma"), "o_dbl": per * ncd if SO else 0}
     em = Emitter()
     out = ['extern "C" __global__ void __launch_bounds__(%d)' % CTA,
            "%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name]
     em("extern __shared__ double sbra[];")
+    if SO:
+        em("double* __restrict__ so = sbra + a.so_off;    // contracted-block accumulators, thread-fastest")
     em("const sqb::WorkItem it = items[blockIdx.x];")
     em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
     em("const sqb::MolRec mr = a.mols[it.mol];        // the molecule of this work item")
@@ -502,9 +509,13 @@ def gen_class_swap(bra, ket, spin, state_max):
     for bi, blk in enumerate(blocks):
         em("case %d: {  // bra functions %s" % (bi, blk))
         em.ind += 1
-        for ab in blk:
-            for cd in range(ncd):
-                em("double o%d_%d = 0;" % (ab, cd))
+        slot = lambda ab, cd: "so[%d * %d + threadIdx.x]" % ((ab - blk[0]) * ncd + cd, CTA)
+        if SO:
+            em("for (int x = 0; x < %d; ++x) so[x * %d + threadIdx.x] = 0.0;" % (len(blk) * ncd, CTA))
+        else:
+            for ab in blk:
+                for cd in range(ncd):
+                    em("double o%d_%d = 0;" % (ab, cd))
         em("for (int j = grp; j < nkp; j += isplit) {")
         em.ind += 1
         em("const double* __restrict__ kj = kprim + j * %d;" % NK)
@@ -559,18 +570,36 @@ def gen_class_swap(bra, ket, spin, state_max):
         em("}")
         # flush with the ket E tables (signed by (-1)^(tau+nu+phi))
         ff = 0
-        for cd in range(ncd):
-            for e, k in enumerate(nz(fk[cd])):
-                sg = "-" if sum(k) % 2 else ""
-                em("{ const double ek = %skj[%d];" % (sg, 5 + offk[cd] + e))
+        if SO:
+            for cd in range(ncd):
+                ks = list(enumerate(nz(fk[cd])))
+                em("{")
+                for e, k in ks:
+                    em("  const double ek%d = %skj[%d];" % (e, "-" if sum(k) % 2 else "", 5 + offk[cd] + e))
                 for ab in blk:
-                    em("  o%d_%d = fma(ek, g%d_%d, o%d_%d);" % (ab, cd, ab, kidx[k], ab, cd))
-                    ff += 2
+                    em("  { double t = %s;" % slot(ab, cd))
+                    for e, k in ks:
+                        em("    t = fma(ek%d, g%d_%d, t);" % (e, ab, kidx[k]))
+                        ff += 2
+                    em("    %s = t; }" % slot(ab, cd))
                 em("}")
+        else:
+            for cd in range(ncd):
+                for e, k in enumerate(nz(fk[cd])):
+                    sg = "-" if sum(k) % 2 else ""
+                    em("{ const double ek = %skj[%d];" % (sg, 5 + offk[cd] + e))
+                    for ab in blk:
+                        em("  o%d_%d = fma(ek, g%d_%d, o%d_%d);" % (ab, cd, ab, kidx[k], ab, cd))
+                        ff += 2
+                    em("}")
         em.ind -= 1
         em("}")
         fl["prim"] += pf
         fl["flush"] += ff
+        if SO:
+            for ab in blk:
+                for cd in range(ncd):
+                    em("const double o%d_%d = %s;" % (ab, cd, slot(ab, cd)))
         qf = emit_digest(em, spin, list(range(ncd)), nab, na, nb_, nd, ablk=blk)
         fl["quartet"] += qf
         em.ind -= 1
@@ -981,11 +1010,11 @@ def main():
             reg.append('   0, nullptr, nullptr, 0, 0, 0, 0,')
         sr, su = r["swap"], u["swap"]
         if sr:
-            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d},' % (
+            reg.append('   %d, (const void*)%s, (const void*)%s, %d, %d, %d, %d},' % (
                 sr["flops"]["passes"], sr["name"], su["name"], sr["flops"]["prim"], sr["flops"]["flush"],
-                sr["flops"]["quartet"]))
+                sr["flops"]["quartet"], sr["flops"]["o_dbl"]))
         else:
-            reg.append('   0, nullptr, nullptr, 0, 0, 0},')
+            reg.append('   0, nullptr, nullptr, 0, 0, 0, 0},')
     reg.append("};")
     reg.append("const int kNumClassKernels = %d;" % (len(metas) // 2))
     reg.append("}  // namespace sqb")

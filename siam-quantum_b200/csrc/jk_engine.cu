@@ -763,10 +763,11 @@ int pick_form(const sqb::ClassKernel& K, bool f32, int uhf, int form, const void
 
 // Shared-memory accumulators of the wide form: the region follows the staged bra primitives.
 void add_acc_region(const sqb::ClassKernel& K, int form_used, SegLaunch& L) {
-  if (form_used != 1 || K.w_o_dbl <= 0) return;
+  const int dbl = form_used == 1 ? K.w_o_dbl : form_used == 2 ? K.s_o_dbl : 0;
+  if (dbl <= 0) return;
   const size_t off = (L.smem + 15) / 16 * 16;
   L.a.so_off = (int)(off / sizeof(double));
-  L.smem = off + (size_t)K.w_o_dbl * L.block.x * sizeof(double);
+  L.smem = off + (size_t)dbl * L.block.x * sizeof(double);
 }
 
 // Raise a kernel's dynamic shared-memory limit once per (device, kernel, size class), so that a

@@ -47,6 +47,7 @@ struct ClassKernel {
   const void* fn_rs;
   const void* fn_us;
   int s_flops_prim, s_flops_flush, s_flops_quartet;
+  int s_o_dbl;            // doubles per thread of the swapped form's shared-memory accumulators (0: registers)
 };
 
 extern const ClassKernel kClassKernels[];
