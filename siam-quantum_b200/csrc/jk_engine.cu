@@ -1048,7 +1048,9 @@ int sqb200_jk_autotune(sqb200_jk* c, const double* dPA, const double* dPB, int r
       double t = 0.0;
       rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, f), st, 2, &t);
       if (rc) return rc;
-      if (f == 0 || t < best) { best = t; bf = f; }
+      // another form replaces the current choice only when clearly faster (3%), so that
+      // near-ties do not flip between runs
+      if (f == 0 || t < 0.97 * best) { best = t; bf = f; }
     }
     c->form[v] = (char)bf;
   }
@@ -1749,7 +1751,7 @@ extern "C" int sqb200_batch_autotune(sqb200_batch* b, const double* dPA, const d
   for (int k = 0; k < sqb::kNumClassKernels; ++k) {
     int bf = 0;
     for (int f = 1; f < 3; ++f)
-      if (has_form(sqb::kClassKernels[k], f) && tf[3 * k + f] < tf[3 * k + bf]) bf = f;
+      if (has_form(sqb::kClassKernels[k], f) && tf[3 * k + f] < 0.97 * tf[3 * k + bf]) bf = f;
     b->form[k] = (char)bf;
   }
   CUDA_OK(cudaStreamSynchronize(st));
