@@ -1,8 +1,9 @@
 """Generate the per-class J/K CUDA kernels (McMurchie-Davidson ERI + fused digestion).
 
 One kernel per quartet class (bra pair class | ket pair class) and spin mode (R: restricted,
-K from PA only; U: unrestricted, K from PA and PB).  A CTA owns one bra shell pair and up to
-128 ket shell pairs: one shell quartet per thread, or per `isplit` threads that each take a
+K from PA only; U: unrestricted, K from PA and PB).  A CTA owns one bra shell pair and as many
+ket shell pairs as it has threads (the runtime launches 32, 64 or 128; the bra staging strides
+by blockDim.x): one shell quartet per thread, or per `isplit` threads that each take a
 strided subset of the bra primitives (the digestion is linear, so each thread digests its
 partial contraction).  For each quartet the threads evaluate
 
