@@ -85,7 +85,8 @@ int sqb200_jk_build_noalloc(sqb200_jk *ctx, const double *dPA, const double *dPB
 /* Counters of the last build: out[0] shell quartets computed, out[1] primitive quartets
  * evaluated, out[2] algorithmic FP64 operations (per-class operation table),
  * out[3] shells, out[4] shell pairs, out[5] kernels the build enqueued.
- * Synchronises the context stream.  (No reference counterpart: instrumentation.) */
+ * Synchronises the context stream; after sqb200_jk_build_device on another stream, call it
+ * once that stream has finished.  (No reference counterpart: instrumentation.) */
 int sqb200_jk_stats(sqb200_jk *ctx, long long *out, int n);
 
 /* Per-class timing: enable (1) or disable (0) CUDA-event timing of every class kernel

@@ -49,6 +49,68 @@ int fail(int code, const std::string& msg) {
       return fail(SQB200_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
+// Host-to-device copy that has landed when it returns.  A plain cudaMemcpy from pageable host
+// memory may return once the data are staged, before the last DMA has reached the device, and
+// the non-blocking streams the kernels run on are not ordered after the legacy stream that
+// copy uses; so every upload goes through the stream it is named for and waits for it.
+inline cudaError_t h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e;
+}
+
+// Device buffers laid out in one allocation, each start 256-byte aligned.  One cudaMalloc and
+// one cudaFree instead of one per buffer: each call changes the GPU's mappings (hundreds of
+// microseconds on a large GPU), and cudaFree synchronises the whole device, stalling every
+// other job that runs on it.
+struct Carve {
+  std::vector<std::pair<void**, size_t>> slots;
+  template <class T>
+  void add(T** dst, size_t bytes) { slots.push_back({(void**)dst, bytes}); }
+  static size_t round(size_t b) { return (std::max<size_t>(b, 1) + 255) / 256 * 256; }
+  size_t bytes() const {
+    size_t tot = 0;
+    for (auto& sl : slots) tot += round(sl.second);
+    return tot;
+  }
+  void place(void* base) {
+    size_t o = 0;
+    for (auto& sl : slots) { *sl.first = (char*)base + o; o += round(sl.second); }
+  }
+  cudaError_t alloc(void** base) {
+    void* p = nullptr;
+    const cudaError_t e = cudaMalloc(&p, std::max<size_t>(bytes(), 256));
+    *base = e == cudaSuccess ? p : nullptr;
+    if (e == cudaSuccess) place(p);
+    return e;
+  }
+};
+
+// A Carve whose buffers are (partly) filled from host arrays: one allocation and one staged
+// host-to-device copy for all of them.
+struct Staged : Carve {
+  std::vector<const void*> src;   // per buffer: its host data, or nullptr (left unset)
+  template <class T>
+  void put(T** dst, size_t bytes, const void* host) { add(dst, bytes); src.push_back(host); }
+  cudaError_t upload(void** base, cudaStream_t st) {
+    src.resize(slots.size(), nullptr);
+    cudaError_t e = alloc(base);
+    if (e != cudaSuccess) return e;
+    size_t o = 0, end = 0;
+    std::vector<size_t> at;
+    for (size_t i = 0; i < slots.size(); ++i) {
+      at.push_back(o);
+      if (src[i] && slots[i].second) end = o + slots[i].second;
+      o += round(slots[i].second);
+    }
+    if (end == 0) return cudaSuccess;
+    std::vector<char> img(end, 0);
+    for (size_t i = 0; i < slots.size(); ++i)
+      if (src[i] && slots[i].second) memcpy(img.data() + at[i], src[i], slots[i].second);
+    return h2d(*base, img.data(), end, st);
+  }
+};
+
 // ---------------------------------------------------------------- Boys table (host)
 
 // F_m(T0) for the grid T0 = g*BOYS_H, m = 0..BOYS_NCOL-1, in long double:
@@ -197,6 +259,9 @@ struct sqb200_jk {
   std::vector<double> schwarz;   // basis level, nbf*nbf
   PairClass cls[sqb::kNumPairClasses];
   cudaStream_t stream = nullptr;
+  void* d_base = nullptr;       // one allocation holding every buffer below
+  void* d_pairbase = nullptr;   // one allocation holding the pair classes' device arrays
+  size_t pairbase_bytes = 0;
   double* d_boys = nullptr;
   int* d_shfirst = nullptr;   // per shell first function
   int* d_shn = nullptr;       // per shell function count
@@ -560,9 +625,8 @@ void build_pairs(sqb200_jk* c) {
 
 int compute_schwarz_device(sqb200_jk* c, double* S_host) {
   const size_t nn = (size_t)c->nbf * c->nbf;
-  double* dS = nullptr;
-  CUDA_OK(cudaMalloc(&dS, nn * sizeof(double)));
-  CUDA_OK(cudaMemset(dS, 0, nn * sizeof(double)));
+  double* dS = c->d_JT;         // scratch: the host-build output buffer, rewritten by every build
+  CUDA_OK(cudaMemsetAsync(dS, 0, nn * sizeof(double), c->stream));
   for (int k = 0; k < sqb::kNumPairClasses; ++k) {
     const PairClass& pc = c->cls[k];
     if (pc.pairs.empty()) continue;
@@ -585,35 +649,52 @@ int compute_schwarz_device(sqb200_jk* c, double* S_host) {
   }
   CUDA_OK(cudaMemcpyAsync(S_host, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_OK(cudaStreamSynchronize(c->stream));
-  CUDA_OK(cudaFree(dS));
   return SQB200_OK;
 }
 
 void free_pairs(sqb200_jk* c) {
+  cudaFree(c->d_pairbase);
+  c->d_pairbase = nullptr;
+  c->pairbase_bytes = 0;
   for (int k = 0; k < sqb::kNumPairClasses; ++k) {
-    cudaFree(c->cls[k].d_primsf);
-    c->cls[k].d_primsf = nullptr;
-  }
-  for (int k = 0; k < sqb::kNumPairClasses; ++k) {
-    cudaFree(c->cls[k].d_pairs);
-    cudaFree(c->cls[k].d_prims);
     c->cls[k].d_pairs = nullptr;
     c->cls[k].d_prims = nullptr;
+    c->cls[k].d_primsf = nullptr;
   }
 }
 
 int upload_pairs(sqb200_jk* c) {
+  Carve cv;
   for (int k = 0; k < sqb::kNumPairClasses; ++k) {
     PairClass& pc = c->cls[k];
     if (pc.pairs.empty()) continue;
-    CUDA_OK(cudaMalloc(&pc.d_pairs, pc.pairs.size() * sizeof(sqb::PairRec)));
-    CUDA_OK(cudaMalloc(&pc.d_prims, pc.prims.size() * sizeof(double)));
-    CUDA_OK(cudaMemcpy(pc.d_pairs, pc.pairs.data(), pc.pairs.size() * sizeof(sqb::PairRec), cudaMemcpyHostToDevice));
-    CUDA_OK(cudaMemcpy(pc.d_prims, pc.prims.data(), pc.prims.size() * sizeof(double), cudaMemcpyHostToDevice));
-    std::vector<float> pf(pc.prims.begin(), pc.prims.end());
-    CUDA_OK(cudaMalloc(&pc.d_primsf, pf.size() * sizeof(float)));
-    CUDA_OK(cudaMemcpy(pc.d_primsf, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    cv.add(&pc.d_pairs, pc.pairs.size() * sizeof(sqb::PairRec));
+    cv.add(&pc.d_prims, pc.prims.size() * sizeof(double));
+    cv.add(&pc.d_primsf, pc.prims.size() * sizeof(float));
   }
+  if (cv.slots.empty()) return SQB200_OK;
+  // the same layout again (the pair lists re-sorted by new Schwarz bounds) reuses the allocation
+  const size_t tot = cv.bytes();
+  if (c->d_pairbase && c->pairbase_bytes != tot) free_pairs(c);
+  if (c->d_pairbase) {
+    cv.place(c->d_pairbase);
+  } else {
+    const cudaError_t e = cv.alloc(&c->d_pairbase);
+    if (e != cudaSuccess) return fail(SQB200_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    c->pairbase_bytes = tot;
+  }
+  // one staged host image of every class's arrays, one copy
+  std::vector<char> img(tot, 0);
+  const char* base = (const char*)c->d_pairbase;
+  for (int k = 0; k < sqb::kNumPairClasses; ++k) {
+    const PairClass& pc = c->cls[k];
+    if (pc.pairs.empty()) continue;
+    memcpy(img.data() + ((const char*)pc.d_pairs - base), pc.pairs.data(), pc.pairs.size() * sizeof(sqb::PairRec));
+    memcpy(img.data() + ((const char*)pc.d_prims - base), pc.prims.data(), pc.prims.size() * sizeof(double));
+    float* pf = (float*)(img.data() + ((const char*)pc.d_primsf - base));
+    for (size_t i = 0; i < pc.prims.size(); ++i) pf[i] = (float)pc.prims[i];
+  }
+  CUDA_OK(h2d(c->d_pairbase, img.data(), tot, c->stream));
   return SQB200_OK;
 }
 
@@ -743,7 +824,7 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
   w.total = (int)items.size();
   if (w.total > 0) {
     CUDA_OK(cudaMalloc(&w.d_items, items.size() * sizeof(sqb::WorkItem)));
-    CUDA_OK(cudaMemcpy(w.d_items, items.data(), items.size() * sizeof(sqb::WorkItem), cudaMemcpyHostToDevice));
+    CUDA_OK(h2d(w.d_items, items.data(), items.size() * sizeof(sqb::WorkItem), c->stream));
   }
   auto ins = c->work.emplace(key, w);
   *out = &ins.first->second;
@@ -981,33 +1062,29 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   std::vector<double> tab = make_boys_table();
   std::vector<int> fst(c->ns), nf(c->ns);
   for (int s = 0; s < c->ns; ++s) { fst[s] = c->shells[s].first; nf[s] = c->shells[s].nfunc; }
-#define ALLOC(p, bytes) do { cudaError_t e_ = cudaMalloc(&(p), (bytes)); if (e_ != cudaSuccess) { sqb200_jk_destroy(c); return fail(SQB200_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e_)); } } while (0)
-  ALLOC(c->d_boys, tab.size() * sizeof(double));
-  ALLOC(c->d_shfirst, c->ns * sizeof(int));
-  ALLOC(c->d_shn, c->ns * sizeof(int));
-  ALLOC(c->d_PA, nn * sizeof(double));
-  ALLOC(c->d_PB, nn * sizeof(double));
-  ALLOC(c->d_PT, nn * sizeof(double));
-  ALLOC(c->d_PM, (size_t)c->ns * c->ns * sizeof(double));
-  ALLOC(c->d_J, nn * sizeof(double));
-  ALLOC(c->d_KA, nn * sizeof(double));
-  ALLOC(c->d_KB, nn * sizeof(double));
-  ALLOC(c->d_JT, nn * sizeof(double));
-  ALLOC(c->d_KAo, nn * sizeof(double));
-  ALLOC(c->d_KBo, nn * sizeof(double));
-  ALLOC(c->d_counters, 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
-  ALLOC(c->d_mol, sizeof(sqb::MolRec));
-#undef ALLOC
-  cudaError_t e = cudaMemcpy(c->d_boys, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(c->d_shfirst, fst.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(c->d_shn, nf.data(), c->ns * sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  Carve cv;
+  cv.add(&c->d_boys, tab.size() * sizeof(double));
+  cv.add(&c->d_shfirst, c->ns * sizeof(int));
+  cv.add(&c->d_shn, c->ns * sizeof(int));
+  for (double** m : {&c->d_PA, &c->d_PB, &c->d_PT, &c->d_J, &c->d_KA, &c->d_KB, &c->d_JT, &c->d_KAo, &c->d_KBo})
+    cv.add(m, nn * sizeof(double));
+  cv.add(&c->d_PM, (size_t)c->ns * c->ns * sizeof(double));
+  cv.add(&c->d_counters, 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
+  cv.add(&c->d_mol, sizeof(sqb::MolRec));
+  cudaError_t e = cv.alloc(&c->d_base);
+  if (e != cudaSuccess) {
+    sqb200_jk_destroy(c);
+    return fail(SQB200_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = h2d(c->d_boys, tab.data(), tab.size() * sizeof(double), c->stream);
+  if (e == cudaSuccess) e = h2d(c->d_shfirst, fst.data(), c->ns * sizeof(int), c->stream);
+  if (e == cudaSuccess) e = h2d(c->d_shn, nf.data(), c->ns * sizeof(int), c->stream);
   if (e != cudaSuccess) { sqb200_jk_destroy(c); return fail(SQB200_ECUDA, cudaGetErrorString(e)); }
   if (!schwarz) {
     // Schwarz bounds from the device, then the pair lists in their final (sorted) order
     rc = compute_schwarz_device(c, c->schwarz.data());
     if (rc) { sqb200_jk_destroy(c); return rc; }
-    free_pairs(c);
     build_pairs(c);
     rc = upload_pairs(c);
     if (rc) { sqb200_jk_destroy(c); return rc; }
@@ -1029,9 +1106,7 @@ int sqb200_jk_destroy(sqb200_jk* c) {
   for (auto& kv : c->work) cudaFree(kv.second.d_items);
   for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   free_pairs(c);
-  void* ptrs[] = {c->d_boys, c->d_shfirst, c->d_shn, c->d_PA, c->d_PB, c->d_PT, c->d_PM, c->d_J, c->d_KA,
-                  c->d_KB, c->d_JT, c->d_KAo, c->d_KBo, c->d_counters, c->d_mol};
-  for (void* p : ptrs) cudaFree(p);
+  cudaFree(c->d_base);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return SQB200_OK;
@@ -1208,35 +1283,62 @@ int sqb200_jk_set_precision(sqb200_jk* c, double fp32_below) {
 }
 
 int sqb200_jk_mem_cutoff(sqb200_jk* c, double fixed, int max_mem_mb, double* out) {
-  // getMemCutoff_Parallel (reference src/matrix.c:3703-3760), nCPU = 1
+  // getMemCutoff_Parallel (reference src/matrix.c:3703-3760), nCPU = 1: starting from `fixed`,
+  // double the cutoff until the shell quartets whose Schwarz product reaches it hold at most
+  // max_mem_mb MB of doubles, step back by half and rise by 5% until they fit again.  The
+  // quartets are the canonical ones, pair(I,J) <= pair(P,Q) in lower-triangle order, and the
+  // reference skips one when S_PQ * S_IJ < cut.  Each count here is exact in
+  // O(pairs log pairs) instead of a pass over all quartets: the pairs sorted by their bound, a
+  // Fenwick tree over that order filled in pair order, and for pair PQ a binary search for the
+  // first sorted bound b with S_PQ * b >= cut (a rounded product is monotonic in b, so the
+  // search selects exactly the quartets the reference keeps).
   if (!c || !out) return fail(SQB200_EINVAL, "null argument");
   const std::vector<Shell>& sh = c->shells;
   const int ns = c->ns;
-  std::vector<double> S((size_t)ns * ns);
-  for (int P = 0; P < ns; ++P)
-    for (int Q = 0; Q < ns; ++Q) {
+  const size_t np = (size_t)ns * (ns + 1) / 2;
+  std::vector<double> sv(np);                    // Schwarz block max per pair, pair order
+  std::vector<unsigned long long> wv(np);        // functions per pair
+  for (int P = 0, k = 0; P < ns; ++P)
+    for (int Q = 0; Q <= P; ++Q, ++k) {
       double r = 0.0;
       for (int p = 0; p < sh[P].nfunc; ++p)
         for (int q = 0; q < sh[Q].nfunc; ++q) r = std::max(r, c->schwarz[(size_t)(sh[P].first + p) * c->nbf + sh[Q].first + q]);
-      S[(size_t)P * ns + Q] = r;
+      sv[k] = r;
+      wv[k] = (unsigned long long)sh[P].nfunc * sh[Q].nfunc;
     }
+  std::vector<int> order(np), rank(np);
+  for (size_t k = 0; k < np; ++k) order[k] = (int)k;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sv[a] < sv[b]; });
+  std::vector<double> vs(np);
+  for (size_t k = 0; k < np; ++k) { rank[order[k]] = (int)k; vs[k] = sv[order[k]]; }
+  std::vector<unsigned long long> fen(np + 1);
   const unsigned long long maxEE = (unsigned long long)max_mem_mb * 1000000ULL / sizeof(double);
+  // true when the quartets kept at `cut` exceed maxEE; *cnt = their function count otherwise
+  auto over = [&](double cut, unsigned long long* cnt) {
+    std::fill(fen.begin(), fen.end(), 0ULL);
+    unsigned long long tot = 0, ins = 0;
+    for (size_t pq = 0; pq < np; ++pq) {
+      for (size_t i = rank[pq] + 1; i <= np; i += i & (~i + 1)) fen[i] += wv[pq];
+      ins += wv[pq];
+      const double s = sv[pq];
+      size_t lo = 0, hi = np;                      // first k with s * vs[k] >= cut
+      while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (s * vs[mid] < cut) lo = mid + 1; else hi = mid;
+      }
+      unsigned long long below = 0;                // inserted weight at ranks < lo
+      for (size_t i = lo; i > 0; i -= i & (~i + 1)) below += fen[i];
+      tot += wv[pq] * (ins - below);
+      if (tot > maxEE) return true;
+    }
+    *cnt = tot;
+    return false;
+  };
   double cut = fixed;
   bool coarse = true;
   for (;;) {
     unsigned long long cnt = 0;
-    bool over = false;
-    for (int P = 0; P < ns && !over; ++P)
-      for (int Q = 0; Q <= P && !over; ++Q)
-        for (int I = 0; I <= P && !over; ++I) {
-          const int N = (I == P) ? Q : I;
-          for (int J = 0; J <= N; ++J) {
-            if (S[(size_t)P * ns + Q] * S[(size_t)I * ns + J] < cut) continue;
-            cnt += (unsigned long long)sh[P].nfunc * sh[Q].nfunc * sh[I].nfunc * sh[J].nfunc;
-            if (cnt > maxEE) { over = true; break; }
-          }
-        }
-    if (over) { cut *= coarse ? 2.00 : 1.05; continue; }
+    if (over(cut, &cnt)) { cut *= coarse ? 2.00 : 1.05; continue; }
     if (coarse && cnt < maxEE) { coarse = false; cut /= 2.0; continue; }
     break;
   }
@@ -1418,34 +1520,28 @@ extern "C" int sqb200_oneint(sqb200_jk* c, int natom, const double* Z, const dou
   const size_t nn = (size_t)n * n;
   int *d_np = nullptr, *d_off = nullptr, *d_lmn = nullptr;
   double *d_xyz = nullptr, *d_ex = nullptr, *d_nc = nullptr, *d_Z = nullptr, *d_A = nullptr, *d_out = nullptr;
-  cudaError_t e = cudaMalloc(&d_np, n * sizeof(int));
-  if (e == cudaSuccess) e = cudaMalloc(&d_off, n * sizeof(int));
-  if (e == cudaSuccess) e = cudaMalloc(&d_lmn, 3 * n * sizeof(int));
-  if (e == cudaSuccess) e = cudaMalloc(&d_xyz, 3 * n * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d_ex, ex.size() * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d_nc, nc.size() * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d_Z, (natom + 1) * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d_A, (3 * natom + 3) * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&d_out, 3 * nn * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemcpy(d_np, np.data(), n * sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_off, off.data(), n * sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_lmn, lmn.data(), 3 * n * sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_xyz, xyz.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_ex, ex.data(), ex.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(d_nc, nc.data(), nc.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && natom > 0) e = cudaMemcpy(d_Z, Z, natom * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess && natom > 0) e = cudaMemcpy(d_A, axyz, 3 * natom * sizeof(double), cudaMemcpyHostToDevice);
+  Staged up;
+  up.put(&d_np, n * sizeof(int), np.data());
+  up.put(&d_off, n * sizeof(int), off.data());
+  up.put(&d_lmn, 3 * n * sizeof(int), lmn.data());
+  up.put(&d_xyz, 3 * n * sizeof(double), xyz.data());
+  up.put(&d_ex, ex.size() * sizeof(double), ex.data());
+  up.put(&d_nc, nc.size() * sizeof(double), nc.data());
+  up.put(&d_Z, natom * sizeof(double), natom > 0 ? Z : nullptr);
+  up.put(&d_A, 3 * natom * sizeof(double), natom > 0 ? axyz : nullptr);
+  up.put(&d_out, 3 * nn * sizeof(double), nullptr);
+  void* base = nullptr;
+  cudaError_t e = up.upload(&base, c->stream);
   if (e == cudaSuccess) {
     k_oneint<<<(int)((nn + 127) / 128), 128, 0, c->stream>>>(n, d_np, d_off, d_lmn, d_xyz, d_ex, d_nc, natom, d_Z, d_A,
                                                               c->d_boys, d_out, d_out + nn, d_out + 2 * nn);
     e = cudaGetLastError();
   }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(S, d_out, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(T, d_out + nn, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(V, d_out + 2 * nn, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  if (e == cudaSuccess) e = cudaMemcpy(S, d_out, nn * sizeof(double), cudaMemcpyDeviceToHost);
-  if (e == cudaSuccess) e = cudaMemcpy(T, d_out + nn, nn * sizeof(double), cudaMemcpyDeviceToHost);
-  if (e == cudaSuccess) e = cudaMemcpy(V, d_out + 2 * nn, nn * sizeof(double), cudaMemcpyDeviceToHost);
-  void* ptrs[] = {d_np, d_off, d_lmn, d_xyz, d_ex, d_nc, d_Z, d_A, d_out};
-  for (void* q : ptrs) cudaFree(q);
+  cudaFree(base);
   if (e != cudaSuccess) return fail(SQB200_ECUDA, std::string("sqb200_oneint: ") + cudaGetErrorString(e));
   return SQB200_OK;
 }
@@ -1600,9 +1696,9 @@ extern "C" int sqb200_batch_create(sqb200_batch** out, int nmol, sqb200_jk* cons
     if (e == cudaSuccess) e = cudaMalloc(&bc.d_prims, prims.size() * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&bc.d_primsf, pf.size() * sizeof(float));
     if (e != cudaSuccess) return bail(SQB200_ENOMEM, cudaGetErrorString(e));
-    e = cudaMemcpy(bc.d_pairs, pairs.data(), pairs.size() * sizeof(sqb::PairRec), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(bc.d_prims, prims.data(), prims.size() * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(bc.d_primsf, pf.data(), pf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    e = h2d(bc.d_pairs, pairs.data(), pairs.size() * sizeof(sqb::PairRec), b->stream);
+    if (e == cudaSuccess) e = h2d(bc.d_prims, prims.data(), prims.size() * sizeof(double), b->stream);
+    if (e == cudaSuccess) e = h2d(bc.d_primsf, pf.data(), pf.size() * sizeof(float), b->stream);
     if (e != cudaSuccess) return bail(SQB200_ECUDA, cudaGetErrorString(e));
   }
   // packed shell tables and per-molecule buffers
@@ -1620,8 +1716,8 @@ extern "C" int sqb200_batch_create(sqb200_batch** out, int nmol, sqb200_jk* cons
   if (e == cudaSuccess) e = cudaMalloc(&b->d_KB, ntot * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 2 * 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
   if (e != cudaSuccess) return bail(SQB200_ENOMEM, cudaGetErrorString(e));
-  e = cudaMemcpy(b->d_shfirst, fst.data(), fst.size() * sizeof(int), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_shn, nf.data(), nf.size() * sizeof(int), cudaMemcpyHostToDevice);
+  e = h2d(b->d_shfirst, fst.data(), fst.size() * sizeof(int), b->stream);
+  if (e == cudaSuccess) e = h2d(b->d_shn, nf.data(), nf.size() * sizeof(int), b->stream);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(SQB200_ECUDA, cudaGetErrorString(e));
   b->form.assign(sqb::kNumClassKernels, 0);
@@ -1663,7 +1759,7 @@ extern "C" int sqb200_batch_set_step(sqb200_batch* b, const int* restricted, con
   }
   CUDA_OK(cudaStreamSynchronize(b->stream));
   for (cudaStream_t s : b->side) CUDA_OK(cudaStreamSynchronize(s));
-  CUDA_OK(cudaMemcpy(b->d_mols, b->rec.data(), b->nmol * sizeof(sqb::MolRec), cudaMemcpyHostToDevice));
+  CUDA_OK(h2d(b->d_mols, b->rec.data(), b->nmol * sizeof(sqb::MolRec), b->stream));
   if (same) return SQB200_OK;
   b->kernel.clear(); b->spin.clear(); b->first.clear(); b->count.clear(); b->cost.clear();
   std::vector<sqb::WorkItem> items, items32;
@@ -1699,7 +1795,7 @@ extern "C" int sqb200_batch_set_step(sqb200_batch* b, const int* restricted, con
     b->items_cap = items.size();
   }
   if (!items.empty())
-    CUDA_OK(cudaMemcpy(b->d_items, items.data(), items.size() * sizeof(sqb::WorkItem), cudaMemcpyHostToDevice));
+    CUDA_OK(h2d(b->d_items, items.data(), items.size() * sizeof(sqb::WorkItem), b->stream));
   b->have_step = true;
   return SQB200_OK;
 }
@@ -1825,6 +1921,7 @@ extern "C" int sqb200_batch_build_device(sqb200_batch* b, const double* dPA, con
 extern "C" int sqb200_batch_stats(sqb200_batch* b, long long* out, int n) {
   if (!b || !out) return fail(SQB200_EINVAL, "null argument");
   CUDA_OK(cudaSetDevice(b->device));
+  CUDA_OK(cudaDeviceSynchronize());      // the build ran on the caller's stream
   const int K_ = sqb::kNumClassKernels;
   std::vector<unsigned long long> h(2 * 8 * K_);
   CUDA_OK(cudaMemcpy(h.data(), b->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -2324,36 +2421,29 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   std::vector<double> PT(nn), PS(nn);
   for (size_t i = 0; i < nn; ++i) { PT[i] = PA[i] + PB[i]; PS[i] = PA[i] - PB[i]; }
   void* d[16] = {nullptr};
-  auto up = [&](int k, const void* h, size_t bytes) -> cudaError_t {
-    cudaError_t e = cudaMalloc(&d[k], bytes ? bytes : 8);
-    if (e == cudaSuccess && bytes) e = cudaMemcpy(d[k], h, bytes, cudaMemcpyHostToDevice);
-    return e;
-  };
-  cudaError_t e = up(0, np.data(), n * sizeof(int));
-  if (e == cudaSuccess) e = up(1, off.data(), n * sizeof(int));
-  if (e == cudaSuccess) e = up(2, lmn.data(), 3 * n * sizeof(int));
-  if (e == cudaSuccess) e = up(3, xyz.data(), 3 * n * sizeof(double));
-  if (e == cudaSuccess) e = up(4, ex.data(), ex.size() * sizeof(double));
-  if (e == cudaSuccess) e = up(5, nc.data(), nc.size() * sizeof(double));
-  if (e == cudaSuccess) e = up(6, fat.data(), n * sizeof(int));
-  if (e == cudaSuccess) e = up(7, Z, natom * sizeof(double));
-  if (e == cudaSuccess) e = up(8, axyz, 3 * natom * sizeof(double));
-  if (e == cudaSuccess) e = up(9, PT.data(), nn * sizeof(double));
-  if (e == cudaSuccess) e = up(10, PS.data(), nn * sizeof(double));
-  if (e == cudaSuccess) e = up(11, W, nn * sizeof(double));
-  if (e == cudaSuccess) e = up(12, gs.data(), ns * sizeof(GShell));
-  if (e == cudaSuccess) e = up(13, sex.data(), sex.size() * sizeof(double));
-  if (e == cudaSuccess) e = up(14, swt.data(), swt.size() * sizeof(double));
-  if (e == cudaSuccess) e = up(15, nullptr, 0);
-  void* dp = nullptr;
-  void *dsch = nullptr, *dpm = nullptr, *dg = nullptr;
-  if (e == cudaSuccess) e = cudaMalloc(&dp, npairs * sizeof(int2));
-  if (e == cudaSuccess) e = cudaMemcpy(dp, pairs.data(), npairs * sizeof(int2), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&dsch, npairs * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemcpy(dsch, psch.data(), npairs * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&dpm, npairs * sizeof(double));
-  if (e == cudaSuccess) e = cudaMemcpy(dpm, ppm.data(), npairs * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMalloc(&dg, 3 * natom * sizeof(double));
+  void *dp = nullptr, *dsch = nullptr, *dpm = nullptr, *dg = nullptr;
+  Staged up;
+  up.put(&d[0], n * sizeof(int), np.data());
+  up.put(&d[1], n * sizeof(int), off.data());
+  up.put(&d[2], 3 * n * sizeof(int), lmn.data());
+  up.put(&d[3], 3 * n * sizeof(double), xyz.data());
+  up.put(&d[4], ex.size() * sizeof(double), ex.data());
+  up.put(&d[5], nc.size() * sizeof(double), nc.data());
+  up.put(&d[6], n * sizeof(int), fat.data());
+  up.put(&d[7], natom * sizeof(double), Z);
+  up.put(&d[8], 3 * natom * sizeof(double), axyz);
+  up.put(&d[9], nn * sizeof(double), PT.data());
+  up.put(&d[10], nn * sizeof(double), PS.data());
+  up.put(&d[11], nn * sizeof(double), W);
+  up.put(&d[12], ns * sizeof(GShell), gs.data());
+  up.put(&d[13], sex.size() * sizeof(double), sex.data());
+  up.put(&d[14], swt.size() * sizeof(double), swt.data());
+  up.put(&dp, npairs * sizeof(int2), pairs.data());
+  up.put(&dsch, npairs * sizeof(double), psch.data());
+  up.put(&dpm, npairs * sizeof(double), ppm.data());
+  up.put(&dg, 3 * natom * sizeof(double), nullptr);
+  void* base = nullptr;
+  cudaError_t e = up.upload(&base, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, 3 * natom * sizeof(double), c->stream);
   if (e == cudaSuccess) {
     if (terms & SQB200_GRAD_ERI)
@@ -2369,8 +2459,7 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   }
   if (e == cudaSuccess) e = cudaMemcpyAsync(grad, dg, 3 * natom * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  for (void* q : d) cudaFree(q);
-  cudaFree(dp); cudaFree(dsch); cudaFree(dpm); cudaFree(dg);
+  cudaFree(base);
   if (e != cudaSuccess) return fail(SQB200_ECUDA, std::string("sqb200_gradient: ") + cudaGetErrorString(e));
   // nuclear repulsion (GradVnn, src/grad.c:43)
   if (terms & SQB200_GRAD_NUCLEAR)

@@ -283,10 +283,12 @@ class SCFJob:
         as numpy arrays, orbital i in row i."""
         out = []
         for F in (self.FA, self.FB):
+            # the copies to the host run on the job's stream, after the products they read
+            # (the default stream is not ordered after it)
             with self._on_stream():
                 w, C = self.torch.linalg.eigh(self.X.T @ F @ self.X)
                 C = (self.X @ C).T
-            out.append((C.cpu().numpy(), w.cpu().numpy()))
+                out.append((C.cpu().numpy(), w.cpu().numpy()))
         return out[0][0], out[1][0], out[0][1], out[1][1]
 
     def gradient(self, terms=15):

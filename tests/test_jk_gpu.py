@@ -161,3 +161,27 @@ def test_c60_full_size_properties():
         cnt += len(pv) - max(j0, i)
     assert st["quartets"] == cnt, (st["quartets"], cnt)
     assert 30e6 < cnt < 40e6                     # survey: 36.2M survivors for C60/6-31G
+
+
+@pytest.mark.gpu
+def test_mem_cutoff_equals_the_reference_rule():
+    """The in-memory cutoff (getMemCutoff, src/matrix.c:3703) is the reference's exact value:
+    the sorted-pair count in the library against the oracle's pass over every quartet, for
+    golden molecules and seeded organics, several cutoffs and memory limits."""
+    sqb = load_sqb200()
+    cases = []
+    for c in GOLDEN_CASES:
+        g = golden(c)
+        cases.append((golden_basis(g), g["schwarz"]))
+    rng = np.random.default_rng(5)
+    for k in (3, 6, 9):
+        b = sqb.basis.build_basis(sqb.molecules.to_bohr(sqb.molecules.random_organic(rng, k)), "631g_star")
+        e = sqb.JKEngine(b)
+        cases.append((b, e.schwarz()))
+        e.close()
+    for b, S in cases:
+        eng = sqb.JKEngine(b, schwarz=S)
+        for cut in (1e-12, 3.7e-11, 1e-9):
+            for mb in (0, 1, 20, 250):
+                assert eng.mem_cutoff(cut, mb) == port.mem_cutoff(b, S, cut, mb), (b.nbf, cut, mb)
+        eng.close()

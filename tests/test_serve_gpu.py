@@ -64,3 +64,30 @@ def test_served_results_equal_alone(two_slots_by_memory):
     # the golden molecules also reach the reference's energies
     for c, o in zip(GOLDEN_CASES, res):
         assert abs(o["energy"] - float(golden(c)["energy"])) <= 1e-8
+
+
+@pytest.mark.gpu
+def test_served_gradients_under_load():
+    """Gradient jobs that finish while many other jobs keep the GPU busy get their alone
+    gradient: every host read of a job's device state is ordered after the job's own stream."""
+    sqb = load_sqb200()
+    rng = np.random.default_rng(29)
+    reqs = []
+    for i in range(10):
+        m = sqb.molecules.random_organic(rng, int(rng.integers(5, 10)))
+        uhf = i % 2 == 1
+        if uhf:
+            m = sqb.molecules.remove_one_h(m, rng)
+        reqs.append({"id": i, "atoms": m, "basis": "631g_star", "charge": 0, "mult": 2 if uhf else 1,
+                     "gradient": True, "arrival": 0.0})
+    srv = sqb.serve.Server(max_active=10)
+    res = srv.run(reqs, realtime=False)
+    assert srv.stats["peak_active"] >= 5
+    checked = 0
+    for r, o in zip(reqs, res):
+        a = sqb.serve.solve_alone(r)
+        if o["converged"] and a[4] is not None:
+            assert abs(o["energy"] - a[0]) <= TOL
+            assert np.abs(o["gradient"] - a[4]).max() <= 1e-8, r["id"]
+            checked += 1
+    assert checked >= 5
