@@ -182,6 +182,25 @@ int sqb200_batch_stats(sqb200_batch *batch, long long *out, int n);
  * stream then), so calls on different streams may overlap. */
 int sqb200_syev_batched(int device, int n, int batch, double *A, double *W, void *stream);
 
+/* Segmented dot products of packed FP64 vectors, for the SCF tail of many molecules: the
+ * density-DIIS matrix B_xy = d_x . d_y of the last four residuals per molecule and the RMS
+ * density change (conv_diis4, src/conv.c:606-844), and the energy sums, over every molecule's
+ * blocks of the packed arrays at once.  A plan fixes nseg segments [seg_start, seg_start +
+ * seg_len) of the vectors and the output slot (0 <= seg_slot < nslot) each one adds to;
+ * sqb200_segdots_run computes out[slot * npair + p] = sum over the slot's segments of
+ * vecs[pair_i[p]][e] * vecs[pair_j[p]][e] (pair_j[p] < 0: vecs[pair_i[p]][e] alone), for
+ * 1 <= nvec <= 4 device vectors (each holding every segment's elements) and 1 <= npair <= 10
+ * products, on `stream`, asynchronously.  The sums are taken in a fixed order (chunks of a
+ * segment, then the chunks of a slot in segment order), so repeated runs agree bit for bit.
+ * Runs of one plan share its scratch: issue them on one stream.  (No reference counterpart:
+ * the reference reduces each molecule on the host.) */
+typedef struct sqb200_segdots sqb200_segdots;
+int sqb200_segdots_create(sqb200_segdots **out, int device, int nseg, const long long *seg_start,
+                          const long long *seg_len, const int *seg_slot, int nslot);
+int sqb200_segdots_run(sqb200_segdots *plan, int nvec, const double *const *vecs, int npair,
+                       const int *pair_i, const int *pair_j, double *out, void *stream);
+int sqb200_segdots_destroy(sqb200_segdots *plan);
+
 /* Gradient of the SCF energy with respect to the natom nuclear positions (bohr), written to
  * grad (natom x 3, hartree/bohr; the reference prints forces = -grad): nuclear repulsion,
  * -sum W dS, sum PT d(T + V) with the Hellmann-Feynman terms, and the two-electron term of

@@ -23,7 +23,7 @@ import numpy as np
 
 from . import basis as B
 from . import molecules as M
-from .engine import JKBatch, JKEngine, syev_batched
+from .engine import JKBatch, JKEngine, SegmentDots, syev_batched
 from .scf import SCF_MAX, DensityDIIS4, electrons, nuclear_repulsion
 
 PAD = 32            # bucket granularity (functions)
@@ -142,6 +142,9 @@ class BatchSCF:
             self.P0 = self.P.clone()
             self.molid = torch.tensor(molid, device=self.dev)
             self.molid2 = torch.cat([self.molid, self.molid])
+            # per-molecule sums over the packed blocks (energy): one pass, fixed order
+            self.edots = SegmentDots([mo["off"] for mo in self.mols], [mo["nbf"] ** 2 for mo in self.mols],
+                                     list(range(nm)), nm, self.dev.index)
             self.nbf2 = torch.tensor([mo["nbf"] ** 2 for mo in self.mols], device=self.dev)
             self.rmask = torch.tensor([mo["restricted"] for mo in self.mols], device=self.dev)[self.molid]
             self.enn = torch.tensor([mo["enn"] for mo in self.mols], **f64)
@@ -160,6 +163,7 @@ class BatchSCF:
         self.iter_count = np.zeros(nm, dtype=np.int64)
         self.iters = 0
         self.graph = None
+        self.diis = None
         self.first = True
         self.build_seconds = 0.0
 
@@ -247,7 +251,7 @@ class BatchSCF:
         Pnew[T_:2 * T_] = torch.where(self.rmask, Pnew[:T_], Pnew[T_:2 * T_])
         PA, PB = Pnew[:T_], Pnew[T_:2 * T_]
         dens = (self.H + 0.5 * self.JT) * (PA + PB) + 0.5 * (self.K[:T_] * PA + self.K[T_:2 * T_] * PB)
-        E = torch.zeros(nm, dtype=torch.float64, device=self.dev).index_add_(0, self.molid, dens) + self.enn
+        E = self.edots([dens], [(0, -1)])[:, 0] + self.enn
         out, avg = self.diis.step(Pnew[:2 * T_])
         keep = self.frozen_t[self.molid2]
         self.Pold.copy_(self.P)
@@ -266,7 +270,11 @@ class BatchSCF:
             ev0.record(self.stream)
             self.frozen = np.zeros(nm, dtype=bool)
             self.frozen_t = torch.zeros(nm, dtype=torch.bool, device=self.dev)
-            self.diis = DensityDIIS4(torch, self.P[:2 * T_], self.molid2, nm, self.nbf2)
+            offs = [mo["off"] for mo in self.mols]
+            lens = [mo["nbf"] ** 2 for mo in self.mols]
+            self.diis = DensityDIIS4(torch, self.P[:2 * T_], self.molid2, nm, self.nbf2,
+                                     segments=(offs + [T_ + o for o in offs], lens + lens,
+                                               list(range(nm)) * 2))
             self._set_step(True)
             self.t_build = self.t_tail = 0.0
             eb0, eb1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -315,6 +323,9 @@ class BatchSCF:
 
     def close(self):
         self.graph = None
+        self.edots.close()
+        if self.diis is not None and self.diis.dots is not None:
+            self.diis.dots.close()
         self.batch.close()
         for e in self.engines:
             e.close()

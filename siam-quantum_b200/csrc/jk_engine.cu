@@ -252,6 +252,11 @@ struct PairClass {
 
 }  // namespace
 
+namespace sqb {
+// The library's error text for the other translation units (sqb200_last_error).
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace sqb
+
 struct sqb200_jk {
   int device = 0;
   int nbf = 0, ns = 0;

@@ -27,6 +27,7 @@ EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_j
            "sqb200_batch_set_step", "sqb200_batch_build_device", "sqb200_batch_stats",
            "sqb200_batch_autotune", "sqb200_jk_autotune", "sqb200_jk_tiles", "sqb200_jk_set_tiles",
            "sqb200_syev_batched", "sqb200_gradient", "sqb200_gradient_terms",
+           "sqb200_segdots_create", "sqb200_segdots_run", "sqb200_segdots_destroy",
            "sqb200_last_error"]
 
 
@@ -74,6 +75,11 @@ def load_library(path=LIB_PATH):
     L.sqb200_gradient.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p]
     L.sqb200_gradient_terms.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p, ctypes.c_int, _f64p]
     L.sqb200_jk_set_tiles.argtypes = [vp, _i32p, ctypes.c_int]
+    _i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+    L.sqb200_segdots_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, _i64p, _i64p, _i32p,
+                                        ctypes.c_int]
+    L.sqb200_segdots_run.argtypes = [vp, ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int, _i32p, _i32p, vp, vp]
+    L.sqb200_segdots_destroy.argtypes = [vp]
     for name in EXPORTS:
         getattr(L, name).restype = ctypes.c_int
     L.sqb200_last_error.restype = ctypes.c_char_p
@@ -250,6 +256,57 @@ def peak_fma(device=0, iters=4096):
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(L.sqb200_peak_fma(device, iters, ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+class SegmentDots:
+    """Per-slot sums of products of packed FP64 CUDA vectors over fixed segments
+    (sqb200_segdots_*): the per-molecule reductions of the SCF tail (DIIS matrix, RMS density
+    change, energy) for many molecules in one pass, in a fixed summation order."""
+
+    def __init__(self, starts, lengths, slots, nslot, device):
+        L = load_library()
+        self.starts = np.ascontiguousarray(starts, dtype=np.int64)
+        self.lengths = np.ascontiguousarray(lengths, dtype=np.int64)
+        self.slots = np.ascontiguousarray(slots, dtype=np.int32)
+        self.nslot = int(nslot)
+        self.device = device
+        self.extent = int((self.starts + self.lengths).max()) if len(self.starts) else 0
+        self._plan = ctypes.c_void_p()
+        _check(L.sqb200_segdots_create(ctypes.byref(self._plan), device, len(self.starts), self.starts,
+                                       self.lengths, self.slots, self.nslot))
+
+    def __call__(self, vecs, pairs, stream=None):
+        """(nslot, len(pairs)) tensor: column p sums vecs[i] * vecs[j] for pairs[p] = (i, j), or
+        vecs[i] alone for j = -1.  `vecs`: 1-4 contiguous FP64 CUDA tensors on the plan's device,
+        each covering every segment; runs on `stream` (default: the current stream)."""
+        import torch
+        if not 1 <= len(vecs) <= 4 or not 1 <= len(pairs) <= 10:
+            raise ValueError("1-4 vectors and 1-10 products")
+        for v in vecs:
+            if (v.dtype != torch.float64 or not v.is_cuda or v.device.index != self.device
+                    or not v.is_contiguous() or v.numel() < self.extent):
+                raise ValueError("vectors must be contiguous FP64 CUDA tensors on device %d with at least %d "
+                                 "elements" % (self.device, self.extent))
+        st = torch.cuda.current_stream(vecs[0].device) if stream is None else stream
+        with torch.cuda.stream(st):
+            out = torch.empty((self.nslot, len(pairs)), dtype=torch.float64, device=vecs[0].device)
+        ptrs = (ctypes.c_void_p * len(vecs))(*[v.data_ptr() for v in vecs])
+        pi = np.array([p[0] for p in pairs], dtype=np.int32)
+        pj = np.array([p[1] for p in pairs], dtype=np.int32)
+        _check(_lib.sqb200_segdots_run(self._plan, len(vecs), ptrs, len(pairs), pi, pj, out.data_ptr(),
+                                       st.cuda_stream))
+        return out
+
+    def close(self):
+        if self._plan:
+            _lib.sqb200_segdots_destroy(self._plan)
+            self._plan = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def syev_batched(A, stream=None):

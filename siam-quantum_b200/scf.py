@@ -63,35 +63,54 @@ class DensityDIIS4:
     5 x 5 DIIS system on the last four residuals (B_xy = sum over both spins of d_x . d_y, rows
     bordered by -1) and return sum_k c_k (P_in,k + d_k), falling back to the damped mix when the
     newest residual grew (B33 > B22).  The RMS deviation sqrt(sum d^2 / nbf^2 / 2) is what
-    the reference tests against SCFConv."""
+    the reference tests against SCFConv.
+
+    On the GPU the per-molecule sums come from the library's segmented dot products
+    (engine.SegmentDots: the ten B entries in one pass, fixed summation order); `segments` =
+    (starts, lengths, slots) lists the contiguous runs of the flat vectors and the molecule
+    each belongs to.  On the CPU (host-logic tests) they are index_add_ sums over `seg`."""
 
     PAIRS = [(0, 0), (0, 1), (0, 2), (0, 3), (1, 1), (1, 2), (1, 3), (2, 2), (2, 3), (3, 3)]
 
-    def __init__(self, torch, P, seg, nseg, nbf2, alpha=SCF_DRAG):
+    def __init__(self, torch, P, seg, nseg, nbf2, alpha=SCF_DRAG, segments=None):
         self.torch = torch
         self.seg, self.nseg, self.alpha = seg, nseg, alpha
         self.nbf2 = nbf2.to(P.dtype)
         self.Pin = [torch.zeros_like(P) for _ in range(3)] + [P.clone()]   # P0, P1, P2, P3
         self.d = [torch.zeros_like(P) for _ in range(4)]                      # dP0 .. dP3
         self.n = 1                                                            # nIter after the first call
+        self.dots = None
+        if P.is_cuda:
+            if segments is None:
+                raise ValueError("DensityDIIS4 on the GPU needs the segments of the packed densities")
+            from .engine import SegmentDots
+            self.dots = SegmentDots(*segments, nseg, P.device.index)
 
     def _segsum(self, x):
         torch = self.torch
         return torch.zeros(self.nseg, dtype=x.dtype, device=x.device).index_add_(0, self.seg, x)
+
+    def _sums(self, ds, pairs):
+        """{(x, y): per-molecule sum of ds[x] * ds[y]}."""
+        if self.dots is not None:
+            S = self.dots(ds, pairs)
+            return {xy: S[:, k] for k, xy in enumerate(pairs)}
+        return {xy: self._segsum(ds[xy[0]] * ds[xy[1]]) for xy in pairs}
 
     def step(self, Pnew):
         """(the next input density, RMS deviation per molecule)."""
         torch = self.torch
         P0, P1, P2, P3 = self.Pin
         d3 = Pnew - P3
-        avg = torch.sqrt(self._segsum(d3 * d3) / self.nbf2 / 2.0)
         d0, d1, d2 = self.d[0], self.d[1], self.d[2]
         a = self.alpha
         if self.n <= 3:
+            avg = torch.sqrt(self._sums([d3], [(0, 0)])[(0, 0)] / self.nbf2 / 2.0)
             out = a * Pnew + (1.0 - a) * P3
         else:
             ds = [d0, d1, d2, d3]
-            Bv = {xy: self._segsum(ds[xy[0]] * ds[xy[1]]) for xy in self.PAIRS}
+            Bv = self._sums(ds, self.PAIRS)
+            avg = torch.sqrt(Bv[(3, 3)] / self.nbf2 / 2.0)
             A = torch.zeros((self.nseg, 5, 5), dtype=Pnew.dtype, device=Pnew.device)
             for (x, y), v in Bv.items():
                 A[:, x, y] = v
@@ -242,7 +261,8 @@ class SCFJob:
             if self.diis is None:
                 self.diis = DensityDIIS4(torch, torch.cat([self.PA.reshape(-1), self.PB.reshape(-1)]),
                                          torch.zeros(2 * n * n, dtype=torch.int64, device=self.dev), 1,
-                                         torch.tensor([n * n], device=self.dev))
+                                         torch.tensor([n * n], device=self.dev),
+                                         segments=([0], [2 * n * n], [0]))
             out, avg = self.diis.step(torch.cat([PA.reshape(-1), PB.reshape(-1)]))
             self.PA = out[:n * n].view(n, n)
             self.PB = self.PA if self.restricted else out[n * n:].view(n, n)
