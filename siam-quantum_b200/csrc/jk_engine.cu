@@ -1013,6 +1013,21 @@ double kernel_flops(const sqb200_jk* c, int v, const unsigned long long* h) {
   return kernel_flops_form(v, f32 || v >= (int)c->ran_form.size() ? 0 : c->ran_form[v], h);
 }
 
+// The autotuner times every form of a class in kTuneRounds interleaved rounds (narrow, wide,
+// swapped, narrow, ...) and keeps each form's fastest round, so that clocks still ramping up at
+// start-up or a stray slow launch do not favour the forms timed later.
+constexpr int kTuneRounds = 3;
+
+// The form to run from the forms' times t[0..2]: the narrow tile unless another form is at
+// least 3% faster than every form before it (near-ties keep the earlier form, so that the
+// choice does not flip between runs).
+int pick_tuned(const sqb::ClassKernel& K, const double* t) {
+  int bf = 0;
+  for (int f = 1; f < 3; ++f)
+    if (has_form(K, f) && t[f] < 0.97 * t[bf]) bf = f;
+  return bf;
+}
+
 // Mean device time (ms) of `reps` launches of L on st after one untimed launch.
 int time_seg(const SegLaunch& L, cudaStream_t st, int reps, double* ms) {
   cudaEvent_t a, b;
@@ -1135,18 +1150,16 @@ int sqb200_jk_autotune(sqb200_jk* c, const double* dPA, const double* dPB, int r
   for (size_t s = 0; s < w->kernel.size(); ++s) {
     const int v = w->kernel[s];
     if (v >= sqb::kNumClassKernels) continue;
-    double best = 0.0;
-    int bf = 0;
-    for (int f = 0; f < 3; ++f) {
-      if (!has_form(sqb::kClassKernels[v], f)) continue;
-      double t = 0.0;
-      rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, f), st, 2, &t);
-      if (rc) return rc;
-      // another form replaces the current choice only when clearly faster (3%), so that
-      // near-ties do not flip between runs
-      if (f == 0 || t < 0.97 * best) { best = t; bf = f; }
-    }
-    c->form[v] = (char)bf;
+    double tf[3] = {0.0, 0.0, 0.0};
+    for (int round = 0; round < kTuneRounds; ++round)
+      for (int f = 0; f < 3; ++f) {
+        if (!has_form(sqb::kClassKernels[v], f)) continue;
+        double t = 0.0;
+        rc = time_seg(seg_single(c, w, s, dPA, dPB, uhf, f), st, 2, &t);
+        if (rc) return rc;
+        tf[f] = round == 0 ? t : std::min(tf[f], t);
+      }
+    c->form[v] = (char)pick_tuned(sqb::kClassKernels[v], tf);
   }
   CUDA_OK(cudaStreamSynchronize(st));
   return SQB200_OK;
@@ -1855,20 +1868,18 @@ extern "C" int sqb200_batch_autotune(sqb200_batch* b, const double* dPA, const d
   for (size_t s = 0; s < b->kernel.size(); ++s) {
     const int v = b->kernel[s];
     if (v >= sqb::kNumClassKernels) continue;
-    for (int f = 0; f < 3; ++f) {
-      if (!has_form(sqb::kClassKernels[v], f)) continue;
-      double t = 0.0;
-      const int rc = time_seg(seg_batch(b, s, dPA, dPB, f), st, 2, &t);
-      if (rc) return rc;
-      tf[3 * v + f] += t;
-    }
+    double ts[3] = {0.0, 0.0, 0.0};
+    for (int round = 0; round < kTuneRounds; ++round)
+      for (int f = 0; f < 3; ++f) {
+        if (!has_form(sqb::kClassKernels[v], f)) continue;
+        double t = 0.0;
+        const int rc = time_seg(seg_batch(b, s, dPA, dPB, f), st, 2, &t);
+        if (rc) return rc;
+        ts[f] = round == 0 ? t : std::min(ts[f], t);
+      }
+    for (int f = 0; f < 3; ++f) tf[3 * v + f] += ts[f];
   }
-  for (int k = 0; k < sqb::kNumClassKernels; ++k) {
-    int bf = 0;
-    for (int f = 1; f < 3; ++f)
-      if (has_form(sqb::kClassKernels[k], f) && tf[3 * k + f] < 0.97 * tf[3 * k + bf]) bf = f;
-    b->form[k] = (char)bf;
-  }
+  for (int k = 0; k < sqb::kNumClassKernels; ++k) b->form[k] = (char)pick_tuned(sqb::kClassKernels[k], &tf[3 * k]);
   CUDA_OK(cudaStreamSynchronize(st));
   return SQB200_OK;
 }
