@@ -797,6 +797,26 @@ void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra
     }
 }
 
+// Launch order inside one class kernel: the CTAs with the longest primitive loop first (a
+// thread runs ceil(bra primitives / isplit) x ket primitives iterations; more kets per item next),
+// so that a launch does not end on a few long CTAs while the rest of the GPU idles.
+// nprims(item) gives the item's (bra, ket) primitive counts.
+template <class F>
+void sort_heavy_first(std::vector<sqb::WorkItem>& v, size_t first, F nprims) {
+  const size_t n = v.size() - first;
+  std::vector<std::pair<long long, size_t>> key(n);
+  for (size_t i = 0; i < n; ++i) {
+    const sqb::WorkItem& it = v[first + i];
+    const std::pair<int, int> np = nprims(it);
+    const long long loop = (long long)((np.first + it.isplit - 1) / it.isplit) * np.second;
+    key[i] = {-(loop * 4096 + it.cnt), i};
+  }
+  std::stable_sort(key.begin(), key.end());
+  std::vector<sqb::WorkItem> tmp(n);
+  for (size_t i = 0; i < n; ++i) tmp[i] = v[first + key[i].second];
+  std::copy(tmp.begin(), tmp.end(), v.begin() + first);
+}
+
 int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) {
   auto key = std::make_tuple(outer, fixed, c->fp32_below);
   auto it = c->work.find(key);
@@ -811,6 +831,13 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
     items32.clear();
     double cost64 = 0.0, cost32 = 0.0;
     class_items(c, ki, outer, fixed, 0, 0, 0, items, items32, cost64, cost32);
+    {
+      const PairClass& B = c->cls[sqb::kClassKernels[ki].bra_cls];
+      const PairClass& T = c->cls[sqb::kClassKernels[ki].ket_cls];
+      auto np = [&](const sqb::WorkItem& it) { return std::make_pair(B.pairs[it.bra].nprim, T.pairs[it.k0].nprim); };
+      sort_heavy_first(items, first, np);
+      sort_heavy_first(items32, 0, np);
+    }
     const int cnt = (int)items.size() - first;
     if (cnt > 0) {
       w.kernel.push_back(ki);
@@ -1792,6 +1819,15 @@ extern "C" int sqb200_batch_set_step(sqb200_batch* b, const int* restricted, con
         if (b->rec[m].uhf != sp) continue;
         class_items(b->mols[m], ki, scf_cutoff[m], fixed_cutoff[m], b->cls[K.bra_cls].pair_base[m],
                     b->cls[K.ket_cls].pair_base[m], m, items, items32, c64, c32);
+      }
+      {
+        auto np = [&](const sqb::WorkItem& it) {
+          const sqb200_jk* mc = b->mols[it.mol];
+          return std::make_pair(mc->cls[K.bra_cls].pairs[it.bra - b->cls[K.bra_cls].pair_base[it.mol]].nprim,
+                                mc->cls[K.ket_cls].pairs[it.k0 - b->cls[K.ket_cls].pair_base[it.mol]].nprim);
+        };
+        sort_heavy_first(items, f64, np);
+        sort_heavy_first(items32, 0, np);
       }
       if ((int)items.size() > f64) {
         b->kernel.push_back(ki); b->spin.push_back(sp); b->first.push_back(f64);
