@@ -326,22 +326,32 @@ __global__ void k_prep(const double* __restrict__ PA, const double* __restrict__
   }
 }
 
-// PM[P][Q] = max over the block of |PT|, |PA|, |PB| (reference src/matrix.c:3894-3904)
-__global__ void k_pmax(const double* __restrict__ PA, const double* __restrict__ PB, const double* __restrict__ PT,
-                       const int* __restrict__ first, const int* __restrict__ nf, int ns, int nbf,
-                       double* __restrict__ PM) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= ns * ns) return;
+// PM[P][Q] = max over the block of |PT|, |PA|, |PB| (reference src/matrix.c:3894-3904).  One
+// warp per shell pair: the lanes share the block's (at most 36) elements, then a warp max (the
+// maximum does not depend on the order, so every launch shape gives the same PM).
+constexpr int kPmaxWarps = 4;
+__global__ void __launch_bounds__(32 * kPmaxWarps) k_pmax(const double* __restrict__ PA, const double* __restrict__ PB,
+                                                         const double* __restrict__ PT, const int* __restrict__ first,
+                                                         const int* __restrict__ nf, int ns, int nbf,
+                                                         double* __restrict__ PM) {
+  const int idx = blockIdx.x * kPmaxWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (idx >= ns * ns) return;                     // whole warps leave together
   const int P = idx / ns, Q = idx % ns;
+  const int np = nf[P], nq = nf[Q], fp = first[P], fq = first[Q];
   double r = 0.0;
-  for (int p = 0; p < nf[P]; ++p)
-    for (int q = 0; q < nf[Q]; ++q) {
-      const int o = (first[P] + p) * nbf + first[Q] + q;
-      r = fmax(r, fabs(PT[o]));
-      r = fmax(r, fabs(PA[o]));
-      r = fmax(r, fabs(PB[o]));
-    }
-  PM[idx] = r;
+  for (int e = lane; e < np * nq; e += 32) {
+    const int p = e / nq, q = e - p * nq;
+    const int o = (fp + p) * nbf + fq + q;
+    r = fmax(r, fmax(fabs(PT[o]), fmax(fabs(PA[o]), fabs(PB[o]))));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  if (lane == 0) PM[idx] = r;
+}
+
+void launch_pmax(const double* PA, const double* PB, const double* PT, const int* first, const int* nf, int ns,
+                 int nbf, double* PM, cudaStream_t st) {
+  k_pmax<<<(ns * ns + kPmaxWarps - 1) / kPmaxWarps, 32 * kPmaxWarps, 0, st>>>(PA, PB, PT, first, nf, ns, nbf, PM);
 }
 
 // JT = J + J^T, KA = -(K + K^T), KB likewise or = KA
@@ -974,7 +984,7 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   if (rc) return rc;
   const sqb::MolRec mv{0, 0, n, c->ns, outer, fixed, dscreen, 0, uhf};
   k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf, c->d_mol, mv);
-  k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM);
+  launch_pmax(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM, st);
   CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 8 * sqb::kNumClassKernels, st));
   c->last_launches = 3 + (int)w->kernel.size();
   // segments largest first, each on the least-loaded lane (lane 0 = st, the others are side
@@ -1173,7 +1183,7 @@ int sqb200_jk_autotune(sqb200_jk* c, const double* dPA, const double* dPB, int r
   const int n = c->nbf, nn = n * n;
   const sqb::MolRec mv{0, 0, n, c->ns, outer, fixed, dscreen, 0, uhf};
   k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf, c->d_mol, mv);
-  k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM);
+  launch_pmax(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM, st);
   for (size_t s = 0; s < w->kernel.size(); ++s) {
     const int v = w->kernel[s];
     if (v >= sqb::kNumClassKernels) continue;
@@ -1511,7 +1521,7 @@ extern "C" int sqb200_jk_build_noalloc(sqb200_jk* c, const double* dPA, const do
   sqb::MolRec* d_mol = (sqb::MolRec*)(base + kNoAllocMolOff);
   const sqb::MolRec mv{0, 0, n, c->ns, outer, fixed, dscreen, 0, uhf};
   k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, PT, J, KA, KB, nn, uhf, d_mol, mv);
-  k_pmax<<<(c->ns * c->ns + 127) / 128, 128, 0, st>>>(dPA, dPB, PT, c->d_shfirst, c->d_shn, c->ns, n, PM);
+  launch_pmax(dPA, dPB, PT, c->d_shfirst, c->d_shn, c->ns, n, PM, st);
   CUDA_OK(cudaMemsetAsync(counters, 0, sizeof(unsigned long long) * 4 * sqb::kNumClassKernels, st));
   for (size_t s = 0; s < kernel.size(); ++s) {
     const sqb::ClassKernel& K = sqb::kClassKernels[kernel[s]];
