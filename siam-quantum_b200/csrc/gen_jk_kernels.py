@@ -70,6 +70,9 @@ G_MAX = int(os.environ.get("SQB_G_MAX", "48"))
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
 F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
 MIN_BLOCKS = int(os.environ.get("SQB_MINB", "0"))   # __launch_bounds__ min CTAs per SM (0 = none)
+# the same bound for the FP64 narrow-tile form only (its state is smallest, so a register cap
+# spills least there); 0 = none
+MIN_BLOCKS_NARROW = int(os.environ.get("SQB_MINB_NARROW", "0"))
 USE_WS = int(os.environ.get("SQB_WS", "0"))   # also emit warp-specialised multi-pass kernels (measured slower on B200; opt-in)
 CTA = 128
 
@@ -219,8 +222,9 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
 
     em = Emitter()
     out = []
+    minb = MIN_BLOCKS_NARROW if (MIN_BLOCKS_NARROW and suffix == "" and not F32) else MIN_BLOCKS
     out.append('extern "C" __global__ void __launch_bounds__(%s)' % (
-        "%d, %d" % (CTA, MIN_BLOCKS) if MIN_BLOCKS else "%d" % CTA))
+        "%d, %d" % (CTA, minb) if minb else "%d" % CTA))
     out.append("%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name)
     if F32:
         em("extern __shared__ float sbra_f32[];")
