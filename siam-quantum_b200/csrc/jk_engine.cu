@@ -2482,10 +2482,29 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
           sm = std::max(sm, c->schwarz[e]);
           pm = std::max(pm, fabs(PA[e] + PB[e]));
         }
-      pairs.push_back(make_int2(P, Q));
+      // the larger shell first ((ab|cd) = (ba|cd); the kernel's result does not depend on it)
+      const Shell &SP = c->shells[P], &SQ = c->shells[Q];
+      const bool swap = std::make_pair(SQ.nfunc, SQ.nprim) > std::make_pair(SP.nfunc, SP.nprim);
+      pairs.push_back(swap ? make_int2(Q, P) : make_int2(P, Q));
       psch.push_back(sm);
       ppm.push_back(pm);
     }
+  // Pairs grouped by shell types and contraction lengths: a thread takes one (bra pair, ket
+  // pair <= bra pair) combination, so neighbouring lanes then run the same loops.  Any order of
+  // the list gives every unique quartet once.
+  {
+    std::vector<int> ord(pairs.size());
+    for (size_t k = 0; k < ord.size(); ++k) ord[k] = (int)k;
+    auto key = [&](int k) {
+      const Shell &X = c->shells[pairs[k].x], &Y = c->shells[pairs[k].y];
+      return std::make_tuple(X.nfunc, Y.nfunc, X.nprim, Y.nprim);
+    };
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return key(a) < key(b); });
+    std::vector<int2> p2(pairs.size());
+    std::vector<double> s2(pairs.size()), m2(pairs.size());
+    for (size_t k = 0; k < ord.size(); ++k) { p2[k] = pairs[ord[k]]; s2[k] = psch[ord[k]]; m2[k] = ppm[ord[k]]; }
+    pairs.swap(p2); psch.swap(s2); ppm.swap(m2);
+  }
   const int npairs = (int)pairs.size();
   if (npairs > 65535) return fail(SQB200_EINVAL, "sqb200_gradient: more than 65535 shell pairs");
   std::vector<double> PT(nn), PS(nn);
