@@ -2179,15 +2179,44 @@ __device__ __forceinline__ double draise(double two_alpha, int i, double up, dou
   return two_alpha * up - (i > 0 ? i * down : 0.0);
 }
 
+__device__ __noinline__ void grad_quartet(int pq, int ij, const int2* __restrict__ pairs,
+                                          const GShell* __restrict__ shells, const double* __restrict__ exps,
+                                          const double* __restrict__ wts, const double* __restrict__ PT,
+                                          const double* __restrict__ PS, int nbf, const double* __restrict__ tab,
+                                          double* sg);
+
+// Two-electron part of the gradient: one block per (bra pair, 128 ket pairs), one thread per
+// unique shell quartet (ket pair index <= bra pair index).
 __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const double* __restrict__ psch,
                            const double* __restrict__ ppm, const GShell* __restrict__ shells,
                            const double* __restrict__ exps, const double* __restrict__ wts,
                            const double* __restrict__ PT, const double* __restrict__ PS, int nbf,
-                           const double* __restrict__ tab, double* __restrict__ grad) {
+                           const double* __restrict__ tab, int natom, double* __restrict__ grad) {
+  // the block's contributions are summed per atom in shared memory first, then added to grad
+  // with one atomic per touched component (grad has only 3 natom entries: atomics of every
+  // thread straight into it collide)
+  extern __shared__ double sgrad[];
   const int pq = blockIdx.y;
+  if (pq >= npairs || (int)(blockIdx.x * blockDim.x) > pq) return;      // whole block: no quartet
+  for (int x = threadIdx.x; x < 3 * natom; x += blockDim.x) sgrad[x] = 0.0;
+  __syncthreads();
   const int ij = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pq >= npairs || ij > pq) return;
-  if (psch[pq] * psch[ij] * ppm[pq] * ppm[ij] < 1e-10) return;
+  const bool live = ij <= pq && !(psch[pq] * psch[ij] * ppm[pq] * ppm[ij] < 1e-10);
+  if (live) grad_quartet(pq, ij, pairs, shells, exps, wts, PT, PS, nbf, tab, sgrad);
+  if (__syncthreads_or(live))
+    for (int x = threadIdx.x; x < 3 * natom; x += blockDim.x) {
+      const double v = sgrad[x];
+      if (v != 0.0) atomicAdd(grad + x, v);
+    }
+}
+
+// One shell quartet (pairs[pq] | pairs[ij]) of k_grad_eri, its contributions added to sg
+// (3 per atom, shared memory).
+__device__ __noinline__ void grad_quartet(int pq, int ij, const int2* __restrict__ pairs,
+                                          const GShell* __restrict__ shells, const double* __restrict__ exps,
+                                          const double* __restrict__ wts, const double* __restrict__ PT,
+                                          const double* __restrict__ PS, int nbf, const double* __restrict__ tab,
+                                          double* sg) {
   const int2 PQ = pairs[pq], IJ = pairs[ij];
   const GShell A = shells[PQ.x], B = shells[PQ.y], C = shells[IJ.x], D = shells[IJ.y];
   const double deg = (PQ.x == PQ.y ? 0.5 : 1.0) * (IJ.x == IJ.y ? 0.5 : 1.0) * (pq == ij ? 0.5 : 1.0);
@@ -2317,10 +2346,10 @@ __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const dou
         }
     }
   for (int x = 0; x < 3; ++x) {
-    atomicAdd(grad + 3 * A.atom + x, g[0][x]);
-    atomicAdd(grad + 3 * B.atom + x, g[1][x]);
-    atomicAdd(grad + 3 * C.atom + x, g[2][x]);
-    atomicAdd(grad + 3 * D.atom + x, -(g[0][x] + g[1][x] + g[2][x]));
+    atomicAdd(sg + 3 * A.atom + x, g[0][x]);
+    atomicAdd(sg + 3 * B.atom + x, g[1][x]);
+    atomicAdd(sg + 3 * C.atom + x, g[2][x]);
+    atomicAdd(sg + 3 * D.atom + x, -(g[0][x] + g[1][x] + g[2][x]));
   }
 }
 
@@ -2490,14 +2519,16 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
       ppm.push_back(pm);
     }
   // Pairs grouped by shell types and contraction lengths: a thread takes one (bra pair, ket
-  // pair <= bra pair) combination, so neighbouring lanes then run the same loops.  Any order of
-  // the list gives every unique quartet once.
+  // pair <= bra pair) combination, so neighbouring lanes then run the same loops; inside a group
+  // the largest Schwarz x density bound first, so that the quartets that pass the screen sit
+  // together and whole warps leave together.  Any order of the list gives every unique quartet
+  // once.
   {
     std::vector<int> ord(pairs.size());
     for (size_t k = 0; k < ord.size(); ++k) ord[k] = (int)k;
     auto key = [&](int k) {
       const Shell &X = c->shells[pairs[k].x], &Y = c->shells[pairs[k].y];
-      return std::make_tuple(X.nfunc, Y.nfunc, X.nprim, Y.nprim);
+      return std::make_tuple(X.nfunc, Y.nfunc, X.nprim, Y.nprim, -(psch[k] * ppm[k]));
     };
     std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return key(a) < key(b); });
     std::vector<int2> p2(pairs.size());
@@ -2536,9 +2567,9 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, 3 * natom * sizeof(double), c->stream);
   if (e == cudaSuccess) {
     if (terms & SQB200_GRAD_ERI)
-      k_grad_eri<<<dim3((npairs + 127) / 128, npairs), 128, 0, c->stream>>>(
+      k_grad_eri<<<dim3((npairs + 127) / 128, npairs), 128, 3 * natom * sizeof(double), c->stream>>>(
           npairs, (const int2*)dp, (const double*)dsch, (const double*)dpm, (const GShell*)d[12], (const double*)d[13],
-          (const double*)d[14], (const double*)d[9], (const double*)d[10], n, c->d_boys, (double*)dg);
+          (const double*)d[14], (const double*)d[9], (const double*)d[10], n, c->d_boys, natom, (double*)dg);
     if (terms & (SQB200_GRAD_HCORE | SQB200_GRAD_OVERLAP))
       k_grad_1e<<<(int)((nn + 127) / 128), 128, 0, c->stream>>>(
           n, (const int*)d[0], (const int*)d[1], (const int*)d[2], (const double*)d[3], (const double*)d[4],
