@@ -11,6 +11,14 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 REFERENCE = "/root/reference"
 
 
+def results_path(name):
+    """Where a GPU test leaves its measured figures as JSON (directory SQB200_TEST_RESULTS,
+    default test_results/ at the repository root, created on first use)."""
+    d = os.environ.get("SQB200_TEST_RESULTS", os.path.join(ROOT, "test_results"))
+    os.makedirs(d, exist_ok=True)
+    return os.path.join(d, name)
+
+
 def load_sqb200():
     """Import the package directory siam-quantum_b200/ as module `sqb200`."""
     if "sqb200" in sys.modules and hasattr(sys.modules["sqb200"], "JKEngine"):

@@ -3,12 +3,11 @@ launch per class kernel must give each molecule exactly its single-molecule buil
 parity-tested against the reference), also when replayed from a captured CUDA graph and after
 the tile autotuner; the batched SCF must reach every molecule's reference energy."""
 import json
-import os
 
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, ROOT, golden, golden_basis, load_sqb200
+from conftest import GOLDEN_CASES, golden, golden_basis, load_sqb200, results_path
 
 TOL_SAME = 1e-12     # batch vs single build of the same molecule (atomic summation order only)
 TOL_REF = 1e-10      # vs the reference's J/K (fixtures)
@@ -146,8 +145,7 @@ def test_batched_scf_reaches_reference_energies():
     iters, secs = bs.iter_count.copy(), bs.seconds
     bs.close()
     err = np.abs(E - np.array([float(g["energy"]) for g in gs]))
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "batched_scf.json"), "w") as f:
+    with open(results_path("batched_scf.json"), "w") as f:
         json.dump({"energies": E.tolist(), "abs_err": err.tolist(), "iters": iters.tolist(), "seconds": secs}, f)
     assert conv.all()
     assert (err <= 1e-8).all(), err

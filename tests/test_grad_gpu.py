@@ -6,12 +6,11 @@ quartets at 1e-10), same densities up to the SCF's convergence: tolerance 1e-9 h
 (measured 1e-13 .. 3e-12).  The test runs several molecules in one process on purpose: a
 kernel that read stack memory it had not written gave right answers only on a fresh context."""
 import json
-import os
 
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, ROOT, golden, load_sqb200
+from conftest import GOLDEN_CASES, golden, load_sqb200, results_path
 
 TOL = 1e-9
 
@@ -27,8 +26,7 @@ def test_gradient_matches_reference_forces(case):
     job.close()
     F = g["force"]
     err = np.abs(G + F).max()
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "grad_%s.json" % case), "w") as f:
+    with open(results_path("grad_%s.json" % case), "w") as f:
         json.dump({"grad": G.tolist(), "ref_force": F.tolist(), "max_abs_err": float(err)}, f)
     assert np.abs(G.sum(axis=0)).max() < 1e-8          # translational invariance
     assert err <= TOL, err

@@ -3,12 +3,11 @@ Boys function, screening and accumulation).  Errors are stated against the plain
 and, through the relinked reference program (which builds with difference densities each
 SCF iteration), against the reference's FP64 SCF energy: the bar is 1e-6 Eh."""
 import json
-import os
 
 import numpy as np
 import pytest
 
-from conftest import ROOT, golden, golden_basis, load_sqb200
+from conftest import golden, golden_basis, load_sqb200, results_path
 from test_dropin_scf import SQREF_GPU, _run
 
 TAUS = [1e-3, 1e-4, 1e-5, 1e-6]
@@ -45,8 +44,7 @@ def test_mixed_error_shrinks_with_tau(case):
         J, K, KB = eng.build(g["PA"], PB, restricted=restricted, scf_cutoff=1e-10)
         assert eng.stats()["quartets"] == q0          # same screening, only precision moves
         errs.append(max(np.abs(J - J0).max(), np.abs(K - K0).max(), np.abs(KB - KB0).max()))
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "mixed_jk_err_%s.json" % case), "w") as f:
+    with open(results_path("mixed_jk_err_%s.json" % case), "w") as f:
         json.dump(dict(zip(map(str, TAUS), errs)), f)
     assert errs[0] < 1e-4
     # monotone above FP64 rounding (1e-13 here); a molecule whose FP32 share is negligible at
@@ -65,6 +63,6 @@ def test_mixed_scf_energy_within_1e6(tau, monkeypatch):
     monkeypatch.setenv("SQB200_FP32_BELOW", str(tau))
     e = _run(SQREF_GPU, g["atoms"], str(g["basis"]), ["-SCFACC=1STEP", "-SCFCONV=1e-8"])
     err = abs(e - float(g["energy"]))
-    with open(os.path.join(ROOT, "gpurun_out", "mixed_scf_err_%g.json" % tau), "w") as f:
+    with open(results_path("mixed_scf_err_%g.json" % tau), "w") as f:
         json.dump({"tau": tau, "energy": e, "reference": float(g["energy"]), "abs_err": err}, f)
     assert err <= 1e-6, err

@@ -1,5 +1,5 @@
-"""bench.py on N GPUs runs N independent replicas (the north star fixes one GPU per build; the
-path is not sharded): the job time is the maximum of the ranks' times and the value counts every
+"""bench.py on N GPUs runs N independent replicas (one build runs on one GPU; the path is not
+sharded): the job time is the maximum of the ranks' times and the value counts every
 rank's work.  Checked here with two gloo ranks on the CPU."""
 import os
 import socket

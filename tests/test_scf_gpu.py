@@ -4,12 +4,11 @@ on the device (GPU J/K of difference densities, the reference's density DIIS, cu
 eigensolves) against the reference's converged energies and iteration counts (uhf(),
 -SCFACC=1STEP -SCFCONV=1e-8)."""
 import json
-import os
 
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, ROOT, golden, golden_basis, load_sqb200
+from conftest import GOLDEN_CASES, golden, golden_basis, load_sqb200, results_path
 
 E_TOL = 1e-8     # Eh, total energy against the reference's uhf() (same loop, same test)
 
@@ -54,8 +53,7 @@ def test_device_scf_energy(case):
     iters, secs = job.iters, job.seconds
     job.close()
     err = abs(e - float(g["energy"]))
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "device_scf_%s.json" % case), "w") as f:
+    with open(results_path("device_scf_%s.json" % case), "w") as f:
         json.dump({"energy": e, "reference": float(g["energy"]), "abs_err": err, "iters": iters,
                    "seconds": secs}, f)
     assert job.converged

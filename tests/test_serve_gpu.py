@@ -5,12 +5,11 @@ alone (same SCF algorithm; only the order of FP64 atomics in the J/K builds diff
 the HBM budget holds only a few jobs at a time.  Tolerance: 1e-9 Eh and the same number of SCF
 iterations (+-1)."""
 import json
-import os
 
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, ROOT, golden, load_sqb200
+from conftest import GOLDEN_CASES, golden, load_sqb200, results_path
 
 TOL = 1e-9
 
@@ -58,8 +57,7 @@ def test_served_results_equal_alone(two_slots_by_memory):
         assert abs(o["iters"] - a[1]) <= 1
         if r.get("gradient"):
             assert np.abs(o["gradient"] - a[4]).max() <= 1e-8
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    with open(os.path.join(ROOT, "gpurun_out", "serve_vs_alone_%d.json" % two_slots_by_memory), "w") as f:
+    with open(results_path("serve_vs_alone_%d.json" % two_slots_by_memory), "w") as f:
         json.dump({"jobs": out, "stats": srv.stats}, f)
     # the golden molecules also reach the reference's energies
     for c, o in zip(GOLDEN_CASES, res):
