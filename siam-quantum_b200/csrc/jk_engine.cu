@@ -2538,6 +2538,8 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   }
   const int npairs = (int)pairs.size();
   if (npairs > 65535) return fail(SQB200_EINVAL, "sqb200_gradient: more than 65535 shell pairs");
+  if (3 * (size_t)natom * sizeof(double) > 48 * 1024)   // per-block atom sums of k_grad_eri
+    return fail(SQB200_EINVAL, "sqb200_gradient: more than 2048 atoms");
   std::vector<double> PT(nn), PS(nn);
   for (size_t i = 0; i < nn; ++i) { PT[i] = PA[i] + PB[i]; PS[i] = PA[i] - PB[i]; }
   void* d[16] = {nullptr};

@@ -333,6 +333,8 @@ class SCFJob:
                             self.avgdP if self.avgdP is not None else 0.0, CA, CB, eA, eB)
 
     def close(self):
+        if self.diis is not None and self.diis.dots is not None:
+            self.diis.dots.close()
         self.eng.close()
 
 
