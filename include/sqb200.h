@@ -68,15 +68,20 @@ int sqb200_jk_build_device(sqb200_jk *ctx, const double *dPA, const double *dPB,
  * the implicit device-wide synchronisation of cudaMalloc/cudaFree.  No counterpart in the
  * reference (an addition of this library).  This call allocates nothing: all its scratch
  * (density sum, block maxima, J/K accumulators, counters, work list) lives in one static
- * device array of about 4 MB that every GPU loading the library keeps until exit.
+ * device array of about 4 MB that every GPU loading the library keeps until exit; its device
+ * address is looked up by sqb200_jk_create, with the context's device current.
  * Limits: nbf <= 256 and at most 65536 work items; larger inputs return SQB200_EINVAL with
- * a message.  The context itself (sqb200_jk_create) must already exist.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  Every call shares the one
- * array, so calls that overlap on the GPU (other streams, other threads, other contexts on
- * the same device) race; serialise them.  Buffers are device pointers on the context's
- * device, enqueued on `stream` (NULL = the context's stream); not synchronised.  Counters of
- * sqb200_jk_stats are not updated by this call. */
+ * a message.  The context itself (sqb200_jk_create) must already exist.  Every call shares
+ * the one array, so calls that overlap on the GPU (other streams, other threads, other
+ * contexts on the same device) race; serialise them.  Buffers are device pointers on the
+ * context's device, enqueued on `stream` (NULL = the context's stream); not synchronised.
+ * The call rebuilds the work list on the host and copies it from host memory on `stream`.
+ * It runs the narrow tile form of every class in 128-thread CTAs on one stream (no autotuned
+ * forms, no FP32 quartets, no side streams), so it is not the fastest build; its throughput
+ * is not measured.  With the CUDA runtime's lazy module loading (the default), the first call
+ * may load kernel code that no earlier call used, which takes device memory for that code;
+ * CUDA_MODULE_LOADING=EAGER loads it at start-up instead.  Counters of sqb200_jk_stats are
+ * not updated by this call. */
 int sqb200_jk_build_noalloc(sqb200_jk *ctx, const double *dPA, const double *dPB,
                             int restricted, double scf_cutoff, double fixed_cutoff,
                             double dscreen_rmax, double *dJT, double *dKA, double *dKB,

@@ -12,6 +12,9 @@
  *                 one FRESH GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3773) after the
  *                 nBasis==0 reset (src/matrix.c:3818), nCPU=1, SCFCutoff=fixedCutoff=cutoff;
  *                 writes JT,KA,KB (3*n*n doubles)
+ *   sqref jkpart  <xyz> <basis> <PA> <PB|-> <restricted> <cutoff> <maxMem> <nCPU> <childID> <out>
+ *                 child childID's share of a fresh build split over nCPU processes, as
+ *                 uhf_getGMatrix (src/uhf.c:132-186) runs it; the caller sums the children
  *   sqref nosymm  <xyz> <basis> <PA> <PB|-> <cutoff> <out>
  *                 GTO_JK_Matrix_NoSymm (src/matrix.c:5098), writes GA,GB
  *   sqref scf     <xyz> <basis> <densout|-> [reference options...]
@@ -128,6 +131,35 @@ int main(int argc, char **argv){
 		double *out[3] = {JT, KA, KB};
 		write_mats(argv[9], n, 3, out);
 		fprintf(stderr, "RESULT nbf=%d seconds=%.6f\n", n, t1 - t0);
+		return 0;
+	}
+
+	if(!strcmp(cmd, "jkpart") && argc >= 12){
+		/* one child's share of a split build, as uhf_getGMatrix (src/uhf.c:132-186) hands it to
+		 * process childID of nCPU: the bra shell pairs PQ with PQ % nCPU == childID
+		 * (src/matrix.c:3909-3910); the caller sums the children's JT/KA/KB */
+		struct GTOBasis_t *g = load_basis(argv[2], argv[3], &n, NULL);
+		double *PA = read_mat(argv[4], n);
+		double *PB = strcmp(argv[5], "-") ? read_mat(argv[5], n) : PA;
+		int restricted = atoi(argv[6]);
+		double cutoff = atof(argv[7]);
+		int maxMem = atoi(argv[8]);
+		int nCPU = atoi(argv[9]), child = atoi(argv[10]);
+		if(nCPU < 1 || child < 0 || child >= nCPU){ fprintf(stderr, "bad nCPU/childID\n"); return 2; }
+		double *S = create_Schwarz(n, g);
+		double *JT = calloc((size_t)n * n, 8), *KA = calloc((size_t)n * n, 8),
+		       *KB = calloc((size_t)n * n, 8);
+		struct option_t opt;
+		char *fa[3] = {"sq", "x", "y"};
+		parse_option(&opt, 3, fa);
+		opt.nCPU = nCPU; opt.maxMem = maxMem; opt.SCFCutoff = cutoff; opt.restricted = restricted;
+		double t0 = now_s();
+		GTO_JK_Matrix_Quartet_Parallel(child, 0, NULL, NULL, NULL, NULL, 0.0, NULL, NULL, NULL, &opt);
+		GTO_JK_Matrix_Quartet_Parallel(child, n, PA, PB, g, S, cutoff, JT, KA, KB, &opt);
+		double t1 = now_s();
+		double *out[3] = {JT, KA, KB};
+		write_mats(argv[11], n, 3, out);
+		fprintf(stderr, "RESULT nbf=%d child=%d ncpu=%d seconds=%.6f\n", n, child, nCPU, t1 - t0);
 		return 0;
 	}
 

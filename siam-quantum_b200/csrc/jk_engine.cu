@@ -306,9 +306,17 @@ struct sqb200_jk {
   std::vector<Ev> events;
   std::vector<double> prof_ms;
   std::vector<long long> prof_launches;
+  // device address of the static scratch array of sqb200_jk_build_noalloc on this context's
+  // device, looked up when the context is created (nullptr + the lookup's error otherwise)
+  unsigned char* noalloc_base = nullptr;
+  cudaError_t noalloc_err = cudaSuccess;
 };
 
 namespace {
+
+// Device address of the static scratch array of sqb200_jk_build_noalloc (defined with it below)
+// on the current device.
+cudaError_t noalloc_lookup(unsigned char** out);
 
 // ---------------------------------------------------------------- device helpers
 
@@ -1149,6 +1157,11 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
     rc = upload_pairs(c);
     if (rc) { sqb200_jk_destroy(c); return rc; }
   }
+  // the scratch array of sqb200_jk_build_noalloc: its device address on this device, looked up
+  // here so that the no-allocation entry point itself does no set-up (a failed lookup only
+  // disables that entry point, which then reports this error)
+  c->noalloc_err = noalloc_lookup(&c->noalloc_base);
+  if (c->noalloc_err != cudaSuccess) (void)cudaGetLastError();
   *out = c;
   return SQB200_OK;
 }
@@ -1427,25 +1440,18 @@ constexpr size_t kNoAllocItemsOff = kNoAllocCountersOff + 4 * kNoAllocMaxKernels
 constexpr size_t kNoAllocMolOff = (kNoAllocItemsOff + (size_t)kNoAllocMaxItems * sizeof(sqb::WorkItem) + 255) / 256 * 256;
 constexpr size_t kNoAllocBytes = kNoAllocMolOff + 256;   // one molecule record
 
+static_assert(sizeof(sqb::MolRec) <= 256, "the molecule record must fit the 256 bytes reserved for it");
+
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {nullptr};
-
-// Device address of the scratch array on the current device (looked up once per device; the
-// host-side symbol itself is not a device address).
-int noalloc_scratch(int device, unsigned char** out) {
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (device < 0 || device >= 64) return fail(SQB200_EINVAL, "device index beyond 63");
-  if (!g_noalloc_addr[device]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || p == nullptr)
-      return fail(SQB200_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_noalloc_addr[device] = p;
-  }
-  *out = (unsigned char*)g_noalloc_addr[device];
-  return SQB200_OK;
+// The host-side symbol g_noalloc_scratch is only a stand-in: its device address on the current
+// device comes from the runtime (called by sqb200_jk_create with the context's device current).
+cudaError_t noalloc_lookup(unsigned char** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e == cudaSuccess && p == nullptr) e = cudaErrorInvalidSymbol;
+  *out = e == cudaSuccess ? (unsigned char*)p : nullptr;
+  return e;
 }
 
 // The work list of the standard kernel form on the host (no device copy kept).
@@ -1501,9 +1507,10 @@ extern "C" int sqb200_jk_build_noalloc(sqb200_jk* c, const double* dPA, const do
                                    std::to_string(kNoAllocMaxNbf));
   if (sqb::kNumClassKernels > kNoAllocMaxKernels) return fail(SQB200_EINVAL, "class table larger than the scratch counters");
   CUDA_OK(cudaSetDevice(c->device));
-  unsigned char* base = nullptr;
-  int rc = noalloc_scratch(c->device, &base);
-  if (rc) return rc;
+  unsigned char* base = c->noalloc_base;
+  if (!base)
+    return fail(SQB200_ECUDA, std::string("sqb200_jk_build_noalloc: no device address for its scratch array: ") +
+                                  cudaGetErrorString(c->noalloc_err));
   thread_local std::vector<sqb::WorkItem> items;
   thread_local std::vector<int> kernel, first, count;
   noalloc_items(c, outer, fixed, items, kernel, first, count);

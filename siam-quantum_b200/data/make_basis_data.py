@@ -65,7 +65,9 @@ def parse_gamess(path):
 
 
 def main():
-    bdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/basis"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_basis_data.py <reference basis directory>")
+    bdir = sys.argv[1]
     data = {name: parse_gamess(os.path.join(bdir, fn)) for name, fn in FILES.items()}
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "basis_sets.json")
     with open(dst, "w") as f:

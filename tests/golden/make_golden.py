@@ -35,7 +35,10 @@ _pkg.__path__ = [os.path.join(ROOT, "siam-quantum_b200")]
 sys.modules.setdefault("sqb200", _pkg)
 from sqb200 import molecules as M  # noqa: E402
 
-BASIS_DIR = "/root/reference/basis"
+# the reference tree (environment variable SQ_REFERENCE): its basis-set files
+if not os.environ.get("SQ_REFERENCE"):
+    sys.exit("make_golden.py: set SQ_REFERENCE to the reference source tree")
+BASIS_DIR = os.path.join(os.environ["SQ_REFERENCE"], "basis")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 

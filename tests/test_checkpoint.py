@@ -9,14 +9,14 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import ROOT, golden, golden_basis, load_oracle, load_sqb200
+from conftest import REFERENCE, ROOT, golden, golden_basis, load_oracle, load_sqb200
 from test_scf_host import OracleJK
 
-BASIS_DIR = "/root/reference/basis"
+BASIS_DIR = os.path.join(REFERENCE, "basis") if REFERENCE else ""
 
 
 def _ref_available():
-    return os.path.exists(os.path.join(ROOT, "oracle", "_ref", "sqref")) and os.path.isdir(BASIS_DIR)
+    return os.path.exists(os.path.join(ROOT, "oracle", "_ref", "sqref")) and bool(BASIS_DIR) and os.path.isdir(BASIS_DIR)
 
 
 def _ref_scf(xyz, bas, *opts):
