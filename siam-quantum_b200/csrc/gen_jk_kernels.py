@@ -68,6 +68,9 @@ SWAP_SMEM_O = int(os.environ.get("SQB_SWAP_SMEM", "0"))
 G_MAX_SWAP = int(os.environ.get("SQB_G_MAX_SWAP", "40"))   # G doubles per pass of that form
 G_MAX = int(os.environ.get("SQB_G_MAX", "48"))
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
+# the wide form stages the ket primitive fields a pass reads in shared memory, one record ahead
+# (cp.async double buffer, thread-private slots), instead of reading them from global memory
+STAGE_WIDE = int(os.environ.get("SQB_STAGE_WIDE", "0"))
 F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
 MIN_BLOCKS = int(os.environ.get("SQB_MINB", "0"))   # __launch_bounds__ min CTAs per SM (0 = none)
 # the same bound for the FP64 narrow-tile form only (its state is smallest, so a register cap
@@ -194,7 +197,7 @@ def n_passes(bra, ket, state_max, smem_o=False):
     return (len(fk) + per - 1) // per
 
 
-def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False):
+def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False, stage=False):
     """Return (kernel source, metadata) for class (bra|ket) and spin 'R' or 'U'.  prec "F"
     emits the mixed form: primitive setup, prefactor cut and Boys function in FP64, Hermite
     integrals, E tables and contracted accumulators in FP32, digestion into the FP64 J/K
@@ -217,8 +220,12 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
     blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
     name = "jk_%s_%s_%s%s%s" % (bra, ket, spin, "_f32" if F32 else "", suffix)
     SO = smem_o and not F32
+    ST = stage and not F32 and not SO and not PREFETCH
+    # ket fields one pass stages: q, Qx, Qy, Qz, prefactor and the pass's E entries
+    nst = 5 + max(sum(len(nz(fk[cd])) for cd in blk) for blk in blocks)
     fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks),
-          "alg_prim": alg_prim_flops(fk, Hb, RT, FMA), "o_dbl": nab * per if SO else 0}
+          "alg_prim": alg_prim_flops(fk, Hb, RT, FMA),
+          "o_dbl": nab * per if SO else (2 * nst if ST else 0)}
 
     em = Emitter()
     out = []
@@ -233,6 +240,10 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
         em("extern __shared__ double sbra[];")
     if SO:
         em("double* __restrict__ so = sbra + a.so_off;    // contracted-block accumulators, thread-fastest")
+    if ST:
+        em("// ket staging slots [2][%d fields][128 threads], thread-fastest (conflict-free reads)" % nst)
+        em("double* __restrict__ stg = sbra + a.so_off + threadIdx.x;")
+        em("const unsigned stg_s = (unsigned)__cvta_generic_to_shared(stg);")
     em("const sqb::WorkItem it = items[blockIdx.x];")
     em("const sqb::PairRec bp = a.bra_pairs[it.bra];")
     em("const sqb::MolRec mr = a.mols[it.mol];        // the molecule of this work item")
@@ -285,6 +296,23 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
             for ab in range(nab):
                 for cd in blk:
                     em("%s o%d_%d = 0;" % (RT, ab, cd))
+        # ket E-table entries this block reads
+        kent = []
+        for cd in blk:
+            for k, (tau, nu, phi) in enumerate(nz(fk[cd])):
+                kent.append((cd, k, offk[cd] + k, -1 if (tau + nu + phi) % 2 else 1))
+        if ST:
+            fields = [0, 1, 2, 3, 4] + [5 + e for (cd, k, e, sg) in kent]
+            def stage_code(jexpr, slotexpr):
+                parts = ["const double* __restrict__ src = kprim + (%s) * %d;" % (jexpr, NK),
+                         "const unsigned dst = stg_s + (unsigned)(%s) * %du;" % (slotexpr, nst * 128 * 8)]
+                for fi, f in enumerate(fields):
+                    parts.append('asm volatile("cp.async.ca.shared.global [%%0], [%%1], 8;" :: "r"(dst + %du), "l"(src + %d) : "memory");' % (fi * 128 * 8, f))
+                return "{ " + " ".join(parts) + " }"
+            # the first record of the sequence (i, j) = (grp, 0), (grp, 1), ..., (grp + isplit, 0), ...
+            em("int slot = 0;")
+            em("if (grp < nbp && nkp > 0) %s" % stage_code("0", "0"))
+            em('asm volatile("cp.async.commit_group;" ::: "memory");')
         em("for (int i = grp; i < nbp; i += isplit) {")
         em.ind += 1
         em("const %s* __restrict__ bi = sbra + i * %d;" % (RT, NB))
@@ -292,11 +320,6 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
         for cd in blk:
             for h in Hb:
                 em("%s g%d_%d = 0;" % (RT, cd, hidx[h]))
-        # ket E-table entries this block reads
-        kent = []
-        for cd in blk:
-            for k, (tau, nu, phi) in enumerate(nz(fk[cd])):
-                kent.append((cd, k, offk[cd] + k, -1 if (tau + nu + phi) % 2 else 1))
         if PREFETCH:
             # two-stage software pipeline: the record of primitive j+1 is loaded while j is
             # computed, and its Boys-table row is fetched at the end of iteration j
@@ -309,7 +332,19 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
             em("}")
         em("for (int j = 0; j < nkp; ++j) {")
         em.ind += 1
-        if PREFETCH:
+        if ST:
+            # the record of the next (i, j) -- it depends on j only -- is copied while this one
+            # is computed; wait_group 1 leaves only that copy in flight
+            em("if (j + 1 < nkp || i + isplit < nbp) %s" % stage_code("j + 1 < nkp ? j + 1 : 0", "slot ^ 1"))
+            em('asm volatile("cp.async.commit_group;" ::: "memory");')
+            em('asm volatile("cp.async.wait_group 1;" ::: "memory");')
+            em("const double* __restrict__ sv = stg + slot * %d;" % (nst * 128))
+            em("slot ^= 1;")
+            em("const double q = sv[0];")
+            em("const double pq = p + q;")
+            em("const double rs = rsqrt(pq);")
+            em("if (TWO_PI_2_5 * kpb * sv[%d] * rs < PRIM_CUTOFF) continue;" % (4 * 128))
+        elif PREFETCH:
             em("const double q = nq, Qx = nQx, Qy = nQy, Qz = nQz, kq = nkq;")
             for (cd, k, e, sg) in kent:
                 em("const %s ek%d_%d = nek%d_%d;" % (RT, cd, k, cd, k))
@@ -330,7 +365,9 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
         if bi == 0:
             em("++nprimq;")   # counted by the pass-0 CTAs only
         em("const double alpha = p * q * (rs * rs);")
-        if PREFETCH:
+        if ST:
+            em("const double X = Px - sv[%d], Y = Py - sv[%d], Z = Pz - sv[%d];" % (128, 256, 384))
+        elif PREFETCH:
             em("const double X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;")
         else:
             em("const double X = Px - kj[1], Y = Py - kj[2], Z = Pz - kj[3];")
@@ -354,7 +391,10 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False)
             em("const %s b%d = %s(w * F[%d]);" % (RT, n, "(float)" if F32 else "", n))
             pf += 1
         # ket E coefficients of this block, signed by (-1)^(tau+nu+phi)
-        if not PREFETCH:
+        if ST:
+            for fi, (cd, k, e, sg) in enumerate(kent):
+                em("const %s ek%d_%d = %ssv[%d];" % (RT, cd, k, "-" if sg < 0 else "", (5 + fi) * 128))
+        elif not PREFETCH:
             for (cd, k, e, sg) in kent:
                 em("const %s ek%d_%d = %skj[%d];" % (RT, cd, k, "-" if sg < 0 else "", 5 + e))
         # consumers of each R value: (cd, k, h) with h + (tau nu phi) = R index
@@ -951,7 +991,7 @@ def main():
                     src.append(s4)
                     m["wide"] = m4
             elif n_passes(bra, ket, STATE_MAX_WIDE) < n_passes(bra, ket, STATE_MAX):
-                s4, m4 = gen_class(bra, ket, spin, "D", STATE_MAX_WIDE, "_w")
+                s4, m4 = gen_class(bra, ket, spin, "D", STATE_MAX_WIDE, "_w", stage=bool(STAGE_WIDE))
                 src.append(s4)
                 m["wide"] = m4
             m["swap"] = None
