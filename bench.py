@@ -6,13 +6,21 @@ the reference's GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3773) in its direct
 (Schwarz cutoff 1e-10, density-weighted screen on every quartet, no integral cache).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload benzene|water|h2co|c60]
+                  [--workload c60|benzene|water|h2co|c60-synthetic|organics|serve]
 
-Default workload: RHF/6-31G* benzene (D6h, C-C 1.39, C-H 1.09 angstrom; 102 functions) from
-its converged SCF density (tests/golden fixture generated by the reference).  c60 = RHF/6-31G
-C60 (540 functions) with a seeded synthetic density and the density screen off (every
-Schwarz survivor computed).  Multi-GPU runs are independent replicas (one molecule's build runs
-on one GPU and is not sharded), value = all ranks' builds / max-over-ranks time.
+Default workload: RHF/6-31G C60 (Ih, 6:6 bonds 1.40, 6:5 bonds 1.45 angstrom; 540 functions)
+from the reference's own converged SCF density (tests/golden/c60_631g.npz, made by running the
+reference), Schwarz 1e-10 and the density screen on every quartet, as the reference's direct
+mode builds it.  benzene = RHF/6-31G* benzene (D6h, C-C 1.39, C-H 1.09 angstrom; 102
+functions) from its converged density; c60-synthetic = C60 with a seeded synthetic density and
+the density screen off.  Multi-GPU runs are independent replicas (one molecule's build runs on
+one GPU and is not sharded), value = all ranks' builds / max-over-ranks time.
+
+The reference arm (--impl reference) and the cpu_baseline of C60 run the reference's own process
+split (oracle/_ref/sqref jkpart: child c of nCPU builds the bra shell pairs PQ with
+PQ % nCPU == c, src/matrix.c:3909-3910) on every host thread: nCPU = threads x SLICES, and
+step k runs the children of slice k mod SLICES, one per thread, so a step is 1/SLICES of a
+build and SLICES consecutive steps make one whole build.
 """
 import argparse
 import importlib.util
@@ -40,6 +48,19 @@ def load_sqb200():
     return mod
 
 
+def c60_reference_density():
+    """C60/6-31G: atoms and the reference's converged RHF density from the fixture (symmetric,
+    stored as its upper triangle)."""
+    g = np.load(os.path.join(ROOT, "tests", "golden", "c60_631g.npz"))
+    n = len(g["nprim"])
+    iu = np.triu_indices(n)
+    P = np.zeros((n, n))
+    P[iu] = g["PA_u"]
+    P = P + np.triu(P, 1).T
+    atoms = [(int(round(a[0])), float(a[1]), float(a[2]), float(a[3])) for a in g["atoms"]]
+    return atoms, P
+
+
 def workload(name, sqb):
     """(atoms_angstrom, basis_name, PA, density_screen, description)"""
     M = sqb.molecules
@@ -52,6 +73,10 @@ def workload(name, sqb):
                 "h2co": "formaldehyde RHF/6-31G* (34 bf)"}[name]
         return atoms, str(g["basis"]), np.array(g["PA"]), True, desc + ", converged density"
     if name == "c60":
+        atoms, PA = c60_reference_density()
+        return (atoms, "631g", PA, True,
+                "C60 RHF/6-31G (Ih, 1.40/1.45 A, 540 bf), the reference's converged density")
+    if name == "c60-synthetic":
         atoms = M.c60()
         b = sqb.basis.build_basis(M.to_bohr(atoms), "631g")
         rng = np.random.default_rng(2024)
@@ -161,6 +186,39 @@ def ref_builds(atoms, basis_name, PA, seconds, procs, sqb):
     return rate, res
 
 
+SLICES = 8                 # steps per whole build in the split reference runs (C60)
+
+
+def ref_split_step(atoms, basis_name, PA, procs, step, sqb):
+    """One step of the reference's own process split of a fresh direct J/K build (MAXMEM=0):
+    nCPU = procs * SLICES children, of which this step runs the procs children of slice
+    step % SLICES concurrently (oracle/_ref/sqref jkpart, one thread each).  Returns the
+    slice's build time: the slowest child's GTO_JK_Matrix_Quartet_Parallel time (reset + build,
+    as the harness times it; process start, basis input and the Schwarz matrix, which the
+    caller computes once per SCF, are outside it)."""
+    sqref = os.path.join(ROOT, "oracle", "_ref", "sqref")
+    if not os.path.exists(sqref):
+        raise FileNotFoundError(sqref)
+    ncpu = procs * SLICES
+    sl = step % SLICES
+    with tempfile.TemporaryDirectory() as d:
+        xyz, bas, pa = _ref_inputs(d, atoms, basis_name, PA, sqb)
+        env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+        ps = [subprocess.Popen([sqref, "jkpart", xyz, bas, pa, "-", "1", "1e-10", "0", str(ncpu),
+                                str(sl * procs + t), os.path.join(d, "o%d.bin" % t)],
+                               stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True, env=env)
+              for t in range(procs)]
+        secs = []
+        for p in ps:
+            _, err = p.communicate()
+            for line in err.splitlines():
+                if line.startswith("RESULT"):
+                    secs.append(float(dict(x.split("=") for x in line.split()[1:])["seconds"]))
+        if len(secs) != procs:
+            raise RuntimeError("reference processes failed")
+    return max(secs)
+
+
 ORG_SEED = 20240601        # seed of the 256-molecule organic set (molecules.organic_set)
 
 
@@ -199,6 +257,25 @@ def ref_scf_sample(mols, basis_name, procs, sqb, timeout=600):
     if any(e is None for e in energies):
         raise RuntimeError("reference SCF failed")
     return wall, energies
+
+
+def ref_scf_iterations(mol, basis_name, sqb, timeout=600):
+    """The reference's own SCF (oracle/_ref/sqref scf, 1STEP, SCFConv 1e-8) of one molecule:
+    (iterations it ran, converged) -- uhf() stops at its iteration cap without converging."""
+    sqref = os.path.join(ROOT, "oracle", "_ref", "sqref")
+    env = dict(os.environ, OPENBLAS_NUM_THREADS="1", OMP_NUM_THREADS="1")
+    with tempfile.TemporaryDirectory() as d:
+        bas = os.path.join(d, "b.txt")
+        with open(bas, "w") as f:
+            f.write(sqb.basis.gamess_text(basis_name, sorted({a[0] for a in mol})))
+        x = os.path.join(d, "m.xyz")
+        with open(x, "w") as f:
+            f.write(sqb.molecules.xyz_text(mol))
+        r = subprocess.run([sqref, "scf", x, bas, "-", "-SCFACC=1STEP", "-SCFCONV=1e-8"], capture_output=True,
+                           text=True, env=env, timeout=timeout)
+    its = [t for t in (ln.split() for ln in r.stdout.splitlines()) if len(t) == 3 and t[0].isdigit() and "E" in t[2]]
+    n = int(its[-1][0]) if its else 0
+    return n, 0 < n < sqb.scf.SCF_MAX
 
 
 def run_organics(args, sqb):
@@ -250,7 +327,9 @@ def run_organics(args, sqb):
         conv.append(int(bs.converged.sum()))
     torch.cuda.synchronize(dev)
     t_max = max_over_ranks(dist, t_dev, dev)
-    value = world * len(mols) * args.steps / t_max
+    # a solve counts only when it met the convergence test (|dE| and RMS dP <= 1e-8) within the
+    # reference's 80 iterations
+    value = world * sum(conv) / t_max
     cv = bs.converged
     dE_rerun = float(np.max(np.abs(bs.energy - E_ref_first)[cv])) if cv.any() else None
     bs_iters = bs.iter_count.copy()
@@ -300,11 +379,22 @@ def run_organics(args, sqb):
                        "l2": "no flush: each step is a whole SCF solve (every iteration rewrites the "
                              "packed %.0f MB density/J/K arrays and the pair data is re-read per class "
                              "launch)" % (8 * tot / 1e6)},
-            "iterations": iters, "converged": conv, "max_abs_dE_between_solves_converged": dE_rerun,
+            "iterations": iters, "converged": conv, "unconverged": [len(mols) - c for c in conv],
+            "max_abs_dE_between_solves_converged": dE_rerun,
             "last_solve_device_split": split,
             "iterations_per_molecule": {"mean": float(np.mean(bs_iters)), "max": int(np.max(bs_iters))},
             "batched_jk": jk, "one_at_a_time_gpu": one, "e2e": e2e, "gpu_launches": None}
     if world == 1 and not args.no_cpu_baseline:
+        # the molecules that did not converge here (<= 120 functions, at most 4): does the
+        # reference's own SCF converge them within its 80 iterations?
+        unc = [i for i in np.nonzero(~cv)[0] if nbfs[i] <= 120][:4]
+        try:
+            line["reference_on_unconverged"] = [
+                {"molecule": int(i), "nbf": nbfs[i], "iterations_here": int(bs_iters[i]),
+                 "reference_iterations": it, "reference_converged": ok}
+                for i, (it, ok) in ((i, ref_scf_iterations(mols[i], bname, sqb)) for i in unc)]
+        except Exception as e:
+            line["reference_on_unconverged"] = "failed: %s" % e
         try:
             small = [i for i, n in enumerate(nbfs) if n <= 120][:16]
             smols = [mols[i] for i in small]
@@ -337,53 +427,68 @@ SERVE_SEED = 20240607       # seed of the served request stream (serve.poisson_r
 
 
 def run_serve(args, sqb):
-    """Served stream: Poisson arrivals of RHF and UHF (doublet) SCF energy jobs, continuous
-    batching on one device; solves/s and p50/p99 latency beside the one-at-a-time GPU path
-    (each job solved alone, FIFO in the same arrival order)."""
+    """Served stream: Poisson arrivals of RHF and UHF (doublet) SCF energy and energy+gradient
+    jobs, continuous batching on one device, at each mean arrival rate of --rates; solves/s
+    (converged solves only) and p50/p99 latency beside the one-at-a-time GPU path (each job
+    solved alone, FIFO in the same arrival order).  `value` is the rate with the highest
+    arrival rate (the saturated throughput)."""
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    reqs = sqb.serve.poisson_requests(SERVE_SEED, args.nreq, args.rate, heavy=(2, args.max_heavy))
+    rates = [float(x) for x in args.rates.split(",")]
     # warm-up: one small job through each path (library load, cuSOLVER handles, kernels' first use)
     warm = sqb.serve.poisson_requests(SERVE_SEED + 1, 3, 100.0, heavy=(2, 4))
-    sqb.serve.Server(device=local, max_active=args.slots).run(warm, realtime=False)
-    srv = sqb.serve.Server(device=local, max_active=args.slots, fp32_below=args.fp32_below)
-    res = srv.run(reqs, realtime=True)
-    lat = np.array([r["latency"] for r in res])
-    alone = [sqb.serve.solve_alone(r, device=local) for r in reqs]
-    dG = [float(np.abs(r["gradient"] - a[4]).max()) for r, a in zip(res, alone)
-          if r["gradient"] is not None and a[4] is not None]
+    sqb.serve.Server(device=local, max_active=args.slots, batched=args.batched).run(warm, realtime=False)
+    # the same molecules at every rate (only the arrival times scale)
+    base = sqb.serve.poisson_requests(SERVE_SEED, args.nreq, 1.0, heavy=(2, args.max_heavy))
+    alone = [sqb.serve.solve_alone(r, device=local) for r in base]
     service = [a[2] + a[3] for a in alone]
-    fifo = np.array(sqb.serve.fifo_latencies([r["arrival"] for r in reqs], service))
-    tf = 0.0
-    for a, sv in sorted(zip([r["arrival"] for r in reqs], service)):
-        tf = max(tf, a) + sv
-    conv = np.array([r["converged"] for r in res])
-    dE = np.array([abs(r["energy"] - a[0]) for r, a in zip(res, alone)])
-    nb = [r["nbf"] for r in res]
-    line = {"metric": "served SCF solves/s", "value": len(reqs) / srv.stats["makespan"], "unit": "solves/s",
-            "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * srv.stats["makespan"],
+    per_rate = []
+    for rate in rates:
+        reqs = [dict(r, arrival=r["arrival"] / rate) for r in base]
+        srv = sqb.serve.Server(device=local, max_active=args.slots, fp32_below=args.fp32_below, batched=args.batched)
+        res = srv.run(reqs, realtime=True)
+        conv = np.array([r["converged"] for r in res])
+        lat = np.array([r["latency"] for r in res])
+        fifo = np.array(sqb.serve.fifo_latencies([r["arrival"] for r in reqs], service))
+        tf = 0.0
+        for a, sv in sorted(zip([r["arrival"] for r in reqs], service)):
+            tf = max(tf, a) + sv
+        conv_alone = np.array([a[1] < sqb.scf.SCF_MAX for a in alone])
+        dE = np.array([abs(r["energy"] - a[0]) for r, a in zip(res, alone)])
+        dG = [float(np.abs(r["gradient"] - a[4]).max()) for r, a in zip(res, alone)
+              if r["gradient"] is not None and a[4] is not None]
+        per_rate.append({
+            "rate_per_s": rate, "solves_per_s": float(conv.sum()) / srv.stats["makespan"],
+            "converged": int(conv.sum()), "unconverged": int((~conv).sum()), "makespan_s": srv.stats["makespan"],
+            "latency_s": {"p50": float(np.percentile(lat[conv], 50)) if conv.any() else None,
+                          "p99": float(np.percentile(lat[conv], 99)) if conv.any() else None},
+            "one_at_a_time_gpu": {"solves_per_s": float(conv_alone.sum()) / tf,
+                                  "p50": float(np.percentile(fifo[conv_alone], 50)) if conv_alone.any() else None,
+                                  "p99": float(np.percentile(fifo[conv_alone], 99)) if conv_alone.any() else None},
+            "served_vs_alone_max_abs_dE": float(dE[conv].max()) if conv.any() else None,
+            "served_vs_alone_max_abs_dgrad": max(dG) if dG else None,
+            "peak_active": srv.stats["peak_active"], "rounds": srv.stats["rounds"]})
+    top = per_rate[-1]
+    nb = [a[5] for a in alone]
+    line = {"metric": "served SCF solves/s", "value": top["solves_per_s"], "unit": "solves/s",
+            "n_gpus": 1, "steps": len(rates), "warmup": 1, "ms_per_step": 1e3 * top["makespan_s"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.fp32_below <= 0 else "f64+f32", "data": "synthetic",
-            "config": {"workload": "%d Poisson arrivals (seed %d, rate %.2f/s) of seeded random organics with "
+            "config": {"workload": "%d Poisson arrivals (seed %d, mean rates %s /s) of seeded random organics with "
                                    "2-%d heavy atoms, 6-31G*, half UHF doublets (one H removed), half energy+"
-                                   "gradient jobs, SCFConv 1e-8" % (len(reqs), SERVE_SEED, args.rate, args.max_heavy),
+                                   "gradient jobs, SCFConv 1e-8" % (len(base), SERVE_SEED, args.rates, args.max_heavy),
                        "nbf_min": min(nb), "nbf_max": max(nb), "nbf_mean": float(np.mean(nb)),
-                       "slots": args.slots, "hbm_budget_bytes": srv.stats["budget_bytes"],
-                       "fp32_below": args.fp32_below, "step": "the whole stream, wall clock from the first "
-                       "arrival's time origin to the last completion",
+                       "slots": args.slots, "fp32_below": args.fp32_below,
+                       "served_builds": "batched (one launch per class over every active job)" if args.batched
+                       else "one build per job on its own stream",
+                       "step": "the whole stream at one rate, wall clock from the first arrival's time origin "
+                               "to the last completion; only converged solves count",
                        "l2": "no flush (each job rewrites its own state every iteration)"},
-            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                          "max": float(lat.max())},
-            "one_at_a_time_gpu": {"solves_per_s": len(reqs) / tf, "p50": float(np.percentile(fifo, 50)),
-                                  "p99": float(np.percentile(fifo, 99)),
-                                  "how": "each request solved alone (set-up + SCF), FIFO in arrival order"},
-            "served_vs_alone_max_abs_dE": float(dE[conv].max()) if conv.any() else None,
-            "converged": int(conv.sum()), "peak_active": srv.stats["peak_active"], "rounds": srv.stats["rounds"],
-            "gradient_jobs": int(sum(1 for r in reqs if r.get("gradient"))),
-            "served_vs_alone_max_abs_dgrad": max(dG) if dG else None,
-            "e2e": {"value": len(reqs) / srv.stats["makespan"], "unit": "solves/s",
+            "rates": per_rate,
+            "gradient_jobs": int(sum(1 for r in base if r.get("gradient"))),
+            "e2e": {"value": top["solves_per_s"], "unit": "solves/s",
                     "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                     "api": "serve.Server.run(requests) from geometries; latency includes queueing and set-up"}}
     print(json.dumps(line), flush=True)
@@ -425,6 +530,8 @@ def run_reference(args, sqb):
         return run_reference_organics(args, sqb)
     atoms, bname, PA, dscreen, desc = workload(args.workload, sqb)
     procs = _cpu_threads()
+    if args.workload == "c60":
+        return run_reference_split(args, atoms, bname, PA, desc, procs, sqb)
     for _ in range(args.warmup):
         ref_builds(atoms, bname, PA, 0, procs, sqb)
     rates, walls = [], []
@@ -447,11 +554,34 @@ def run_reference(args, sqb):
     return 0
 
 
+def run_reference_split(args, atoms, bname, PA, desc, procs, sqb):
+    """Reference arm of the C60 build: the reference's own process split (ref_split_step),
+    W + K steps, each step 1/SLICES of a whole build on every host thread."""
+    for k in range(args.warmup):
+        ref_split_step(atoms, bname, PA, procs, k, sqb)
+    secs = [ref_split_step(atoms, bname, PA, procs, args.warmup + k, sqb) for k in range(args.steps)]
+    value = args.steps / SLICES / sum(secs)
+    line = {"metric": METRIC, "value": value, "unit": "builds/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * float(np.mean(secs)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": desc, "screen": "Schwarz 1e-10 + density (direct, MAXMEM=0)",
+                       "parallelism": "the reference's own split: %d processes of nCPU=%d per step, "
+                                      "%d steps per build" % (procs, procs * SLICES, SLICES)},
+            "cpu_baseline": {"value": value, "unit": "builds/s", "cores": procs, "kind": "reference",
+                             "sample": "each step: children [s*%d, (s+1)*%d) of nCPU=%d of a fresh direct build "
+                                       "(oracle/_ref/sqref jkpart, gcc -O3), s = step %% %d" % (
+                                           procs, procs, procs * SLICES, SLICES)},
+            "e2e": {"value": value, "unit": "builds/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant class
 # kernel, from one `ncu --set full` capture of the same workload; the summary with its command
 # is profiles/<kernel>_<workload>.md.  Kernels without a capture report null.
 TRAFFIC = {("benzene", "jk_DL_LL_R"): 912384, ("benzene", "jk_DL_LL_R_w"): 845312,
-           ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60", "jk_LL_LL_R_w"): 18592768}
+           ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768}
 
 
 def max_over_ranks(dist, t_local, device):
@@ -586,7 +716,7 @@ def run_ours(args, sqb):
     if tb is not None and not dom32:
         roof["traffic"] = tb
         roof["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/%s" % (
-            {"benzene": "jk_DL_LL_R_forms_benzene_631gs.md", "c60": "jk_LL_LL_R_w_c60_631g.md"}.get(
+            {"benzene": "jk_DL_LL_R_forms_benzene_631gs.md", "c60-synthetic": "jk_LL_LL_R_w_c60_631g.md"}.get(
                 args.workload, args.workload))
     line = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
@@ -594,6 +724,7 @@ def run_ours(args, sqb):
             "dtype": "f64" if args.fp32_below <= 0 else "f64+f32", "data": "synthetic",
             "config": {"workload": desc, "nbf": n, "fp32_below": args.fp32_below, "screen": "Schwarz 1e-10 + density" if dscreen else "Schwarz 1e-10",
                        "parallelism": "replicas x%d" % world, "l2": "256 MB write between timed builds (untimed)",
+                       "launch": "persistent work queue" if args.persistent else "one CTA per work unit",
                        "quartets_per_build": st["quartets"], "prim_quartets_per_build": st["prim_quartets"],
                        "tiles": ("autotuned forms per class: %d narrow, %d wide, %d swapped" % (
                            int((tiles == 0).sum()), int((tiles == 1).sum()), int((tiles == 2).sum()))
@@ -605,7 +736,20 @@ def run_ours(args, sqb):
                                 "tflops": r["flops"] / (r["ms"] / r["launches"] / 1e3) / 1e12}
                                for r in prof), key=lambda x: -x["ms_per_build"])[:6]}
 
-    if world == 1 and not (args.no_cpu_baseline or args.profile_run):
+    if world == 1 and not (args.no_cpu_baseline or args.profile_run) and args.workload == "c60":
+        try:
+            procs = _cpu_threads()
+            nst = 4
+            secs = [ref_split_step(atoms, bname, PA_np, procs, k, sqb) for k in range(nst)]
+            line["cpu_baseline"] = {"value": nst / SLICES / sum(secs), "unit": "builds/s", "cores": procs,
+                                    "kind": "reference",
+                                    "sample": "%d of the %d slices of one fresh direct build split over nCPU=%d "
+                                              "reference processes (oracle/_ref/sqref jkpart), %d at a time" % (
+                                                  nst, SLICES, procs * SLICES, procs)}
+        except Exception as e:  # the GPU line is still valid without the baseline
+            line["cpu_baseline"] = {"value": None, "unit": "builds/s", "cores": 0, "kind": "reference",
+                                    "sample": "failed: %s" % e}
+    elif world == 1 and not (args.no_cpu_baseline or args.profile_run):
         try:
             procs = _cpu_threads()
             rate, res = ref_builds(atoms, bname, PA_np, args.cpu_seconds, procs, sqb)
@@ -631,17 +775,21 @@ def main():
     ap.add_argument("--warmup", type=int, default=None,
                     help="untimed steps (default 5 builds; 1 batch of solves for organics)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="benzene", choices=["benzene", "water", "h2co", "c60", "organics", "serve"])
+    ap.add_argument("--workload", default="c60",
+                    choices=["c60", "benzene", "water", "h2co", "c60-synthetic", "organics", "serve"])
     ap.add_argument("--nmol", type=int, default=256, help="molecules of the organics workload")
-    ap.add_argument("--nreq", type=int, default=48, help="requests of the serve workload")
-    ap.add_argument("--rate", type=float, default=2.0, help="mean arrival rate (1/s) of the serve workload")
-    ap.add_argument("--max-heavy", type=int, default=20, help="largest molecule (heavy atoms) of the serve workload")
+    ap.add_argument("--nreq", type=int, default=32, help="requests of the serve workload")
+    ap.add_argument("--rates", default="0.5,1,2", help="mean arrival rates (1/s) of the serve workload")
+    ap.add_argument("--batched", type=int, default=1, help="serve: batched Fock builds over the active jobs")
+    ap.add_argument("--max-heavy", type=int, default=40, help="largest molecule (heavy atoms) of the serve workload")
     ap.add_argument("--slots", type=int, default=32, help="concurrent jobs of the serve workload")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep every class on its narrow tile")
     ap.add_argument("--fp32-below", type=float, default=0.0,
                     help="mixed precision: quartets with Schwarz product below this run in FP32")
+    ap.add_argument("--persistent", action="store_true",
+                    help="class kernels as persistent work-queue launches (SQB200_PERSISTENT=1)")
     ap.add_argument("--profile-run", action="store_true",
                     help="minimal run for ncu launch lists: no clock tail, 1 e2e step, no CPU baseline")
     args = ap.parse_args()
@@ -650,6 +798,8 @@ def main():
         args.steps = 1 if args.workload == "organics" else 50
     if args.warmup is None:
         args.warmup = 1 if args.workload == "organics" else 5
+    if args.persistent:
+        os.environ["SQB200_PERSISTENT"] = "1"       # read by every context at creation
     sqb = load_sqb200()
     if args.impl == "reference":
         return run_reference(args, sqb)

@@ -116,6 +116,27 @@ const char *sqb200_jk_class_name(int k);
  * counterpart: the reference computes every quartet in FP64. */
 int sqb200_jk_set_precision(sqb200_jk *ctx, double fp32_below);
 
+/* Reference-parity multipole mode (enable = 1) for the following builds of the context: the
+ * reference's monopole substitution of GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3945-3949,
+ * computeQuartetMPole :2609, getErrExpQuartetMPole :2551, genMultipole src/multipole.c:33).
+ * The context keeps, per shell quartet surviving the outer Schwarz cutoff, the base-1.5
+ * exponent of the largest error of the monopole-monopole approximation, measured the first
+ * time the quartet is computed; a later build takes the monopole values for a quartet with
+ * Sch(PQ)*Sch(IJ) < cache_rmax (the reference's memory cutoff: it never substitutes the
+ * quartets it caches) whose 1.5^exponent * maxPShell is below fixed_cutoff.  With the
+ * reference's cutoff schedule (-SCFACC=3STEP, its default) this reproduces the reference's
+ * energies, approximation included.  Builds run the narrow FP64 form with one thread per
+ * quartet (no FP32 quartets, no autotuned forms).  enable = 0 returns to exact quartets. */
+int sqb200_jk_set_multipole(sqb200_jk *ctx, int enable, double cache_rmax);
+
+/* Persistent work-queue launches (enable = 1) for the following builds: every class kernel runs
+ * as a grid of at most one CTA per resident slot of the GPU (occupancy x SMs) whose CTAs take the
+ * launch's work units -- (work item, pass), heaviest items first -- from a device counter until
+ * none is left, instead of one CTA per unit.  Results are the same either way (up to the order
+ * of floating-point atomics).  Default: the environment variable SQB200_PERSISTENT=1 at context
+ * creation, else off.  (No reference counterpart: launch shape.) */
+int sqb200_jk_set_persistent(sqb200_jk *ctx, int enable);
+
 /* Tile autotuner.  Every class has up to three FP64 forms: 0 the narrow tile (ket functions
  * split into passes of at most 64 accumulator doubles), 1 the wide tile (fewer, larger passes;
  * classes with several passes only), 2 the swapped loop roles (outer loop over the thread's own
@@ -173,6 +194,10 @@ int sqb200_batch_build_device(sqb200_batch *batch, const double *dPA, const doub
 /* The tile autotuner of sqb200_jk_autotune on a batch's work list of the current step (each
  * class keeps the form whose summed time over both spins is lower). */
 int sqb200_batch_autotune(sqb200_batch *batch, const double *dPA, const double *dPB, void *stream);
+
+/* Persistent work-queue launches for the batch's builds (see sqb200_jk_set_persistent; a new
+ * batch starts with the setting of its first context). */
+int sqb200_batch_set_persistent(sqb200_batch *batch, int enable);
 
 /* Counters of the last batched build, as sqb200_jk_stats (summed over molecules).
  * Synchronises with the device. */

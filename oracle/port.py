@@ -135,6 +135,22 @@ def ref_jk(xyz_path, basis_path, PA, PB=None, restricted=True, cutoff=1e-10, max
     return m[0], m[1], m[2], res
 
 
+def ref_jkseq(xyz_path, basis_path, densities, cutoffs, scf_cutoff=1e-10, max_mem=250):
+    """Visits of one reference SCF (sqref jkseq): after a reset, one restricted
+    GTO_JK_Matrix_Quartet_Parallel per (density, fixedCutoff), its cached state carried from
+    visit to visit.  Returns a list of (JT, KA) per visit."""
+    n = densities[0].shape[0]
+    with tempfile.TemporaryDirectory() as d:
+        args = ["jkseq", xyz_path, basis_path, 1, "%.17g" % scf_cutoff, max_mem, os.path.join(d, "out.bin")]
+        for v, (P, c) in enumerate(zip(densities, cutoffs)):
+            pth = os.path.join(d, "p%d.bin" % v)
+            np.ascontiguousarray(P, dtype=np.float64).tofile(pth)
+            args += [pth, "%.17g" % c]
+        ref_run(args)
+        m = np.fromfile(os.path.join(d, "out.bin")).reshape(len(densities), 3, n, n)
+    return [(m[v, 0], m[v, 1]) for v in range(len(densities))]
+
+
 def ref_scf(xyz_path, basis_path, options=()):
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "dens.bin")

@@ -15,6 +15,9 @@
  *   sqref jkpart  <xyz> <basis> <PA> <PB|-> <restricted> <cutoff> <maxMem> <nCPU> <childID> <out>
  *                 child childID's share of a fresh build split over nCPU processes, as
  *                 uhf_getGMatrix (src/uhf.c:132-186) runs it; the caller sums the children
+ *   sqref jkseq   <xyz> <basis> <restricted> <scfCutoff> <maxMem> <out> <P1> <cut1> [<P2> <cut2> ...]
+ *                 visits of one SCF after a reset: one build per (density, fixedCutoff), the
+ *                 reference's cached state carried between them; JT,KA,KB per visit
  *   sqref nosymm  <xyz> <basis> <PA> <PB|-> <cutoff> <out>
  *                 GTO_JK_Matrix_NoSymm (src/matrix.c:5098), writes GA,GB
  *   sqref scf     <xyz> <basis> <densout|-> [reference options...]
@@ -160,6 +163,44 @@ int main(int argc, char **argv){
 		double *out[3] = {JT, KA, KB};
 		write_mats(argv[11], n, 3, out);
 		fprintf(stderr, "RESULT nbf=%d child=%d ncpu=%d seconds=%.6f\n", n, child, nCPU, t1 - t0);
+		return 0;
+	}
+
+	if(!strcmp(cmd, "jkseq") && argc >= 10 && (argc - 8) % 2 == 0){
+		/* a sequence of visits of one SCF: the reset, then GTO_JK_Matrix_Quartet_Parallel
+		 * (nCPU=1) once per (density, fixedCutoff) pair with the reference's state (eeBank,
+		 * erBank, firstVisit) carried from visit to visit, as uhf() calls it through
+		 * uhf_getGMatrix (src/uhf.c:1596) with the zeroed outputs it passes (src/uhf.c:124-129);
+		 * writes JT,KA,KB of every visit */
+		struct GTOBasis_t *g = load_basis(argv[2], argv[3], &n, NULL);
+		int restricted = atoi(argv[4]);
+		double scfcut = atof(argv[5]);
+		int maxMem = atoi(argv[6]);
+		int nv = (argc - 8) / 2;
+		double *S = create_Schwarz(n, g);
+		struct option_t opt;
+		char *fa[3] = {"sq", "x", "y"};
+		parse_option(&opt, 3, fa);
+		opt.nCPU = 1; opt.maxMem = maxMem; opt.SCFCutoff = scfcut; opt.restricted = restricted;
+		GTO_JK_Matrix_Quartet_Parallel(0, 0, NULL, NULL, NULL, NULL, 0.0, NULL, NULL, NULL, &opt);
+		FILE *f = fopen(argv[7], "wb");
+		if(!f){ fprintf(stderr, "cannot write %s\n", argv[7]); exit(2); }
+		double *JT = calloc((size_t)n * n, 8), *KA = calloc((size_t)n * n, 8),
+		       *KB = calloc((size_t)n * n, 8);
+		for(int v = 0; v < nv; v++){
+			double *PA = read_mat(argv[8 + 2 * v], n);
+			double cut = atof(argv[9 + 2 * v]);
+			memset(JT, 0, sizeof(double) * n * n);
+			memset(KA, 0, sizeof(double) * n * n);
+			memset(KB, 0, sizeof(double) * n * n);
+			GTO_JK_Matrix_Quartet_Parallel(0, n, PA, PA, g, S, cut, JT, KA, KB, &opt);
+			fwrite(JT, sizeof(double), (size_t)n * n, f);
+			fwrite(KA, sizeof(double), (size_t)n * n, f);
+			fwrite(KB, sizeof(double), (size_t)n * n, f);
+			free(PA);
+		}
+		fclose(f);
+		fprintf(stderr, "RESULT nbf=%d visits=%d\n", n, nv);
 		return 0;
 	}
 

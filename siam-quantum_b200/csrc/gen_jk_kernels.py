@@ -221,6 +221,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     name = "jk_%s_%s_%s%s%s" % (bra, ket, spin, "_f32" if F32 else "", suffix)
     SO = smem_o and not F32
     ST = stage and not F32 and not SO and not PREFETCH
+    MP = not F32 and suffix == "" and not SO   # the narrow FP64 form carries the multipole mode
     # ket fields one pass stages: q, Qx, Qy, Qz, prefactor and the pass's E entries
     nst = 5 + max(sum(len(nz(fk[cd])) for cd in blk) for blk in blocks)
     fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks),
@@ -259,17 +260,29 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     em("bool ok = kl < it.cnt;")
     em("sqb::PairRec kp = bp;")
     em("double deg = 0.0;")
+    if MP:
+        em("bool mpq = false;                            // multipole mode: the quartet takes monopole values")
+        em("int erx = -1, erexp = sqb::ERR_UNKNOWN;      // its error-bank slot and stored exponent")
     em("if (ok) {")
     em.ind += 1
     em("kp = a.ket_pairs[it.k0 + kl];")
     em("const double r = bp.schwarz * kp.schwarz;")
     em("ok = !(r < mr.cut_outer) && !(r < mr.cut_fixed);")
-    em("if (ok && r < mr.dscreen_rmax) {")
+    if MP:
+        em("if (ok && a.erbank) { erx = a.er_items[blockIdx.x] + kl; erexp = a.erbank[erx]; }")
+        em("const bool mpc = erexp != sqb::ERR_UNKNOWN && r < a.mp_rmax;   // substitution candidate")
+        em("if (ok && (r < mr.dscreen_rmax || mpc)) {")
+    else:
+        em("if (ok && r < mr.dscreen_rmax) {")
     em("  const bool bf = (bp.P > kp.P) || (bp.P == kp.P && bp.Q >= kp.Q);")
     em("  const int P = bf ? bp.P : kp.P, Q = bf ? bp.Q : kp.Q, I = bf ? kp.P : bp.P, J = bf ? kp.Q : bp.Q;")
     em("  const double* PM = a.PM + mr.pmoff; const int ns = mr.ns;")
     em("  const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];")
-    em("  ok = !(r * mp < mr.cut_fixed);")
+    if MP:
+        em("  if (r < mr.dscreen_rmax) ok = !(r * mp < mr.cut_fixed);")
+        em("  if (ok && mpc) mpq = a.pow15[erexp - sqb::ERR_MIN] * mp < mr.cut_fixed;")
+    else:
+        em("  ok = !(r * mp < mr.cut_fixed);")
     em("}")
     em("deg = (bp.P == bp.Q ? 0.5 : 1.0) * (kp.P == kp.Q ? 0.5 : 1.0) * ((a.same_class && it.bra == it.k0 + kl) ? 0.5 : 1.0);")
     em.ind -= 1
@@ -280,7 +293,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     em("if (ok) {")
     em.ind += 1
     em("const %s* __restrict__ kprim = a.ket_prims%s + kp.poff;" % (RT, "_f" if F32 else ""))
-    em("const int nbp = bp.nprim, nkp = kp.nprim;")
+    em("const int nbp = %sbp.nprim, nkp = kp.nprim;" % ("mpq ? 0 : " if MP else ""))
     em("nflush = pass == 0 ? (unsigned long long)((nbp - grp + isplit - 1) / isplit) : 0ull;")
     em("const double* __restrict__ PA = a.PA + mr.moff;")
     if spin == "U":
@@ -437,6 +450,8 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
         em("}")
         fl["prim"] += pf
         fl["flush"] += ff
+        if MP:
+            emit_multipole(em, blk, nab, nb_, nd)
         # digestion of this block
         if SO:
             for ab in range(nab):
@@ -461,11 +476,41 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     em("sqb::count_add(a.counters + 1, nprimq);")
     em("sqb::count_add(a.counters + 2, nflush);")
     em("sqb::count_add(a.counters + 3, (ok && pass == 0) ? 1ull : 0ull);")
-    out.extend(em.lines)
+    out.extend(persistent_body(em.lines))
     out.append("}")
     meta = {"name": name, "bra": bra, "ket": ket, "spin": spin, "nab": nab, "ncd": ncd,
             "neb": len(layb), "nek": len(layk), "Lt": Lt, "flops": fl}
     return "\n".join(out) + "\n", meta
+
+
+def persistent_body(lines):
+    """Wrap a class kernel's body in the work loop of the persistent launch.  A work unit is one
+    (work item, pass) pair.  With a.queue null the CTA runs the unit (blockIdx.x, blockIdx.y)
+    and stops (one CTA per unit); otherwise a grid of about one CTA per resident slot takes
+    units from the device counter a.queue -- unit q is item q / npass, pass q % npass, heaviest
+    items first as the work list orders them -- until the a.nqueue units are taken."""
+    body = [l.replace("blockIdx.x", "qi_").replace("blockIdx.y", "qp_") for l in lines]
+    out = ["  __shared__ int q_next;",
+           "  const bool persistent = a.queue != nullptr;",
+           "  for (int round = 0;; ++round) {",
+           "    int qi_, qp_;",
+           "    if (persistent) {",
+           "      __syncthreads();                  // the previous unit is done with shared memory",
+           "      if (threadIdx.x == 0) q_next = (int)atomicAdd(a.queue, 1ull);",
+           "      __syncthreads();",
+           "      const int q = q_next;",
+           "      if (q >= a.nqueue) break;",
+           "      qi_ = q / a.npass;",
+           "      qp_ = q - qi_ * a.npass;",
+           "    } else {",
+           "      if (round > 0) break;",
+           "      qi_ = blockIdx.x;",
+           "      qp_ = blockIdx.y;",
+           "    }",
+           "    {"]
+    out += ["    " + l for l in body]
+    out += ["    }", "  }"]
+    return out
 
 
 def swap_worthwhile(bra, ket):
@@ -663,11 +708,37 @@ def gen_class_swap(bra, ket, spin, state_max):
     em("sqb::count_add(a.counters + 1, nprimq);")
     em("sqb::count_add(a.counters + 2, nflush);")
     em("sqb::count_add(a.counters + 3, (ok && pass == 0) ? 1ull : 0ull);")
-    out.extend(em.lines)
+    out.extend(persistent_body(em.lines))
     out.append("}")
     meta = {"name": name, "bra": bra, "ket": ket, "spin": spin, "nab": nab, "ncd": ncd,
             "neb": len(layb), "nek": len(layk), "Lt": pair_L(bra) + pair_L(ket), "flops": fl}
     return "\n".join(out) + "\n", meta
+
+
+def emit_multipole(em, blk, nab, nb_, nd):
+    """Multipole mode of the narrow FP64 form: a substituted quartet (mpq) takes the monopole
+    values of computeQuartetMPole (reference src/matrix.c:2609-2647) for its block; an exactly
+    computed quartet whose exponent is still unknown contributes the largest |exact - monopole|
+    over its block (getErrExpQuartetMPole, src/matrix.c:2551-2600) to its error-bank slot,
+    combined over the passes by an atomic maximum of the bits (non-negative doubles order as
+    integers; bit 63 marks the slot as measured)."""
+    em("if (mpq) {")
+    em("  const int fP = bp.fP, fQ = bp.fQ, fI = kp.fP, fJ = kp.fQ;")
+    for ab in range(nab):
+        aa, bb = divmod(ab, nb_)
+        for cd in blk:
+            c, d = divmod(cd, nd)
+            em("  o%d_%d = sqb::mpole_value(a.mpole, N, fP + %d, fQ + %d, fI + %d, fJ + %d);" % (ab, cd, aa, bb, c, d))
+    em("} else if (erexp == sqb::ERR_UNKNOWN && a.erbank) {")
+    em("  const int fP = bp.fP, fQ = bp.fQ, fI = kp.fP, fJ = kp.fQ;")
+    em("  double e = 0.0;")
+    for ab in range(nab):
+        aa, bb = divmod(ab, nb_)
+        for cd in blk:
+            c, d = divmod(cd, nd)
+            em("  e = fmax(e, fabs(o%d_%d - sqb::mpole_value(a.mpole, N, fP + %d, fQ + %d, fI + %d, fJ + %d)));" % (ab, cd, aa, bb, c, d))
+    em("  atomicMax(a.erscr + erx, (unsigned long long)__double_as_longlong(e) | (1ull << 63));")
+    em("}")
 
 
 def emit_digest(em, spin, blk, nab, na, nb_, nd, ablk=None):

@@ -73,7 +73,41 @@ struct JKArgs {
                                // accumulator slots of the shared-memory wide form
   const float* bra_prims_f;    // FP32 copies of the primitive records (mixed-precision kernels)
   const float* ket_prims_f;
+  // Reference-parity multipole mode (erbank == nullptr: off; narrow FP64 form, isplit 1).
+  // The reference's GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3914-3967) keeps, per shell
+  // quartet surviving the outer Schwarz cutoff, the base-1.5 exponent of the largest error of
+  // the monopole approximation (getErrExpQuartetMPole, src/matrix.c:2551), measured the first
+  // time the quartet is computed; on later visits a quartet below its memory cutoff whose
+  // 1.5^exponent * maxPShell is below the fixed cutoff takes the monopole values instead
+  // (computeQuartetMPole, src/matrix.c:2609).
+  signed char* erbank;         // per outer-cutoff survivor: exponent, or ERR_UNKNOWN
+  unsigned long long* erscr;   // per survivor: bits of this build's largest error | 1 << 63
+  const int* er_items;         // per work item: erbank index of its first ket
+  const double* mpole;         // per function pair (p * nbf + q): charge q, centre x, y, z
+  const double* pow15;         // 1.5^e, e = -120..120, as the host's pow computes it
+  double mp_rmax;              // quartets with Sch(PQ)*Sch(IJ) >= this are never substituted
+  // Persistent launch (queue != nullptr): a fixed grid takes the nqueue work units (item, pass)
+  // of the launch from this device counter, zeroed before the launch; npass passes per item.
+  unsigned long long* queue;
+  int nqueue, npass;
 };
+
+constexpr int ERR_MIN = -120;      // src/matrix.c:1745-1747
+constexpr int ERR_MAX = 120;
+constexpr int ERR_UNKNOWN = 121;
+#define MULTIPOLE_R2_CUTOFF 1.0    // src/multipole.h:23: below this squared distance the term is 0
+
+// Monopole-monopole value of the function-pair quartet (pq|rs) (computeQuartetMPole): charges
+// times the inverse distance between the pairs' charge centres, 0 when the squared distance
+// is below MULTIPOLE_R2_CUTOFF; the same operations in the same order, without contractions.
+__device__ __forceinline__ double mpole_value(const double* __restrict__ mp, int N, int p, int q, int r, int s) {
+  const double* m1 = mp + 4 * ((long long)p * N + q);
+  const double* m2 = mp + 4 * ((long long)r * N + s);
+  const double dx = __dadd_rn(m1[1], -m2[1]), dy = __dadd_rn(m1[2], -m2[2]), dz = __dadd_rn(m1[3], -m2[3]);
+  const double K = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  if (K < MULTIPOLE_R2_CUTOFF) return 0.0;
+  return __dmul_rn(__dmul_rn(m1[0], m2[0]), __dsqrt_rn(__ddiv_rn(1.0, K)));
+}
 
 // F_0..F_M at T.  M is a compile-time order so the recursion unrolls.
 template <int M>

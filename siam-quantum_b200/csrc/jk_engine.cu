@@ -274,6 +274,8 @@ struct sqb200_jk {
   double *d_J = nullptr, *d_KA = nullptr, *d_KB = nullptr;
   double *d_JT = nullptr, *d_KAo = nullptr, *d_KBo = nullptr;   // outputs for host builds
   unsigned long long* d_counters = nullptr;  // 4 per class kernel form
+  unsigned long long* d_queue = nullptr;     // persistent launches: work-unit counter per kernel form
+  bool persistent = false;                   // class kernels as persistent work-queue launches
   sqb::MolRec* d_mol = nullptr;              // the build's molecule record (written by k_prep)
   // work lists cached per (outer, fixed) cutoff
   // a segment's kernel index v < K is the FP64 form of class v, v >= K the FP32 form of
@@ -283,9 +285,11 @@ struct sqb200_jk {
     std::vector<int> first, count;
     std::vector<double> cost;     // estimated FP operations per segment (launch order, stream choice)
     sqb::WorkItem* d_items = nullptr;
+    int* d_er = nullptr;          // multipole mode: per item, the error-bank slot of its first ket
     int total = 0;
   };
-  std::map<std::tuple<double, double, double>, Work> work;
+  // key: outer cutoff, fixed cutoff, FP32 threshold, multipole mode
+  std::map<std::tuple<double, double, double, int>, Work> work;
   double fp32_below = 0.0;      // quartets with Schwarz product below this use the FP32 form
   bool use_ws = true;           // warp-specialised form where a class has one (SQB200_WS=0 disables)
   std::vector<char> ran_ws;     // per class kernel: which form the last build launched
@@ -310,6 +314,19 @@ struct sqb200_jk {
   // device, looked up when the context is created (nullptr + the lookup's error otherwise)
   unsigned char* noalloc_base = nullptr;
   cudaError_t noalloc_err = cudaSuccess;
+  // reference-parity multipole mode (sqb200_jk_set_multipole): monopole table, powers of 1.5,
+  // and the error bank, one slot per quartet that survives the outer Schwarz cutoff, laid out
+  // in work-list order for that cutoff (er_outer) and kept from build to build
+  bool mp_on = false;
+  double mp_rmax = 0.0;
+  void* d_mpbase = nullptr;             // one allocation: d_mpole, d_pow15
+  double* d_mpole = nullptr;
+  double* d_pow15 = nullptr;
+  void* d_erbase = nullptr;             // one allocation: d_erscr, d_erbank
+  unsigned long long* d_erscr = nullptr;
+  signed char* d_erbank = nullptr;
+  long long er_total = -1;
+  double er_outer = -1.0;
 };
 
 namespace {
@@ -372,6 +389,24 @@ __global__ void k_finalize(const double* __restrict__ J, const double* __restric
     const double ka = -(KA[i] + KA[t]);
     KAo[i] = ka;
     if (KBo) KBo[i] = uhf ? -(KB[i] + KB[t]) : ka;
+  }
+}
+
+// Multipole mode: every bank slot still unknown that this build measured (scratch bit 63) takes
+// the reference's exponent of the largest error, (signed char) clamp(log(maxErr) * LNBASEI)
+// with ERROR_MIN for an exact zero (getErrExpQuartetMPole, src/matrix.c:2594-2599); the
+// scratch is cleared for the next build.
+__global__ void k_erbank(signed char* __restrict__ bank, unsigned long long* __restrict__ scr, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long v = scr[i];
+    if (!v) continue;
+    scr[i] = 0ull;
+    if (bank[i] != sqb::ERR_UNKNOWN) continue;
+    const double e = __longlong_as_double((long long)(v & ~(1ull << 63)));
+    double x = e == 0.0 ? (double)sqb::ERR_MIN : log(e) * 2.4663034624;   // LNBASEI, 1/ln(1.5)
+    if (x < sqb::ERR_MIN) x = sqb::ERR_MIN;
+    if (x > sqb::ERR_MAX) x = sqb::ERR_MAX;
+    bank[i] = (signed char)x;
   }
 }
 
@@ -760,14 +795,18 @@ int ensure_side_streams(sqb200_jk* c) {
 // operations, the launch-order and stream-balancing estimate.
 void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra_base, int ket_base, int mol,
                  std::vector<sqb::WorkItem>& items, std::vector<sqb::WorkItem>& items32, double& cost64,
-                 double& cost32) {
+                 double& cost32, std::vector<int>* ers = nullptr, long long* er_run = nullptr) {
   const sqb::ClassKernel& K = sqb::kClassKernels[ki];
   const PairClass& B = c->cls[K.bra_cls];
   const PairClass& T = c->cls[K.ket_cls];
   if (B.pairs.empty() || T.pairs.empty()) return;
   const double cut = std::max(outer, fixed);
   const bool same = K.bra_cls == K.ket_cls;
-  const bool mixed = c->fp32_below > 0.0 && K.fn_r32 != nullptr;
+  // multipole mode (er_run != nullptr): FP64 narrow form with one thread per quartet, and every
+  // item records the error-bank slot of its first ket; the slots of each (bra, ket sub-list)
+  // run are the outer-cutoff survivors in order, so the layout does not depend on `fixed`
+  const bool mpm = er_run != nullptr;
+  const bool mixed = !mpm && c->fp32_below > 0.0 && K.fn_r32 != nullptr;
   // every (bra sub-list, ket sub-list) combination; inside one class each unordered pair of
   // sub-lists once, and inside one sub-list each unordered pair of pairs once (k >= b)
   for (size_t sx = 0; sx + 1 < B.sub.size(); ++sx)
@@ -779,7 +818,7 @@ void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra
       // (the warp-specialised form takes 32 kets per CTA, one lane each)
       const bool ws = c->use_ws && K.ws_r != nullptr;
       int isplit = 1;
-      while (!ws && isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
+      while (!ws && !mpm && isplit * 2 <= nbp && isplit * 2 <= 32 && (long)nbp * nkp / (isplit * 2) >= 32) isplit *= 2;
       const int kper = ws ? 32 : cta_threads() / isplit;
       const double pq = (double)nbp * nkp;
       for (int b = b0; b < b1; ++b) {
@@ -794,6 +833,18 @@ void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra
         }
         const int end = lo;
         const int start = (same && sx == sy) ? b : k0s;
+        long long er0 = 0;
+        if (mpm) {
+          // outer-cutoff survivors of this run: the bank slots er0 .. er0 + count - 1
+          const double tho = outer / sb * (1.0 - 1e-12);
+          int lo2 = k0s, hi2 = k1s;
+          while (lo2 < hi2) {
+            const int m2 = (lo2 + hi2) / 2;
+            if (T.pairs[m2].schwarz >= tho) lo2 = m2 + 1; else hi2 = m2;
+          }
+          er0 = *er_run;
+          *er_run += std::max(0, lo2 - start);
+        }
         // kets with Sch(bra)*Sch(ket) >= fp32_below (a prefix) stay FP64, the rest go FP32
         int mid = end;
         if (mixed) {
@@ -805,8 +856,10 @@ void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra
           }
           mid = l2;
         }
-        for (int k0 = start; k0 < mid; k0 += kper)
+        for (int k0 = start; k0 < mid; k0 += kper) {
           items.push_back({bra_base + b, ket_base + k0, std::min(kper, mid - k0), isplit, mol});
+          if (mpm) ers->push_back((int)(er0 + (k0 - start)));
+        }
         for (int k0 = std::max(start, mid); k0 < end; k0 += kper)
           items32.push_back({bra_base + b, ket_base + k0, std::min(kper, end - k0), isplit, mol});
         cost64 += std::max(0, mid - start) * (pq * K.flops_prim + K.flops_quartet);
@@ -836,7 +889,8 @@ void sort_heavy_first(std::vector<sqb::WorkItem>& v, size_t first, F nprims) {
 }
 
 int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) {
-  auto key = std::make_tuple(outer, fixed, c->fp32_below);
+  const int mpm = c->mp_on ? 1 : 0;
+  auto key = std::make_tuple(outer, fixed, mpm ? 0.0 : c->fp32_below, mpm);
   auto it = c->work.find(key);
   if (it != c->work.end()) {
     *out = &it->second;
@@ -844,12 +898,15 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
   }
   sqb200_jk::Work w;
   std::vector<sqb::WorkItem> items, items32;
+  std::vector<int> ers;
+  long long er_run = 0;
   for (int ki = 0; ki < sqb::kNumClassKernels; ++ki) {
     const int first = (int)items.size();
     items32.clear();
     double cost64 = 0.0, cost32 = 0.0;
-    class_items(c, ki, outer, fixed, 0, 0, 0, items, items32, cost64, cost32);
-    {
+    class_items(c, ki, outer, fixed, 0, 0, 0, items, items32, cost64, cost32, mpm ? &ers : nullptr,
+                mpm ? &er_run : nullptr);
+    if (!mpm) {   // (multipole mode keeps the items with their bank slots in generation order)
       const PairClass& B = c->cls[sqb::kClassKernels[ki].bra_cls];
       const PairClass& T = c->cls[sqb::kClassKernels[ki].ket_cls];
       auto np = [&](const sqb::WorkItem& it) { return std::make_pair(B.pairs[it.bra].nprim, T.pairs[it.k0].nprim); };
@@ -875,6 +932,28 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
   if (w.total > 0) {
     CUDA_OK(cudaMalloc(&w.d_items, items.size() * sizeof(sqb::WorkItem)));
     CUDA_OK(h2d(w.d_items, items.data(), items.size() * sizeof(sqb::WorkItem), c->stream));
+  }
+  if (mpm) {
+    if (er_run > INT_MAX) return fail(SQB200_EINVAL, "multipole mode: more than 2^31 quartets survive the outer cutoff");
+    if (!ers.empty()) {
+      CUDA_OK(cudaMalloc(&w.d_er, ers.size() * sizeof(int)));
+      CUDA_OK(h2d(w.d_er, ers.data(), ers.size() * sizeof(int), c->stream));
+    }
+    // the bank: laid out for this outer cutoff; a new outer cutoff starts a new bank
+    if (c->er_outer != outer || c->er_total != er_run) {
+      if (c->d_erbase) { cudaFree(c->d_erbase); c->d_erbase = nullptr; }
+      const size_t ns = (size_t)std::max<long long>(1, er_run);
+      Carve cv;
+      cv.add(&c->d_erscr, ns * sizeof(unsigned long long));
+      cv.add(&c->d_erbank, ns);
+      cudaError_t e = cv.alloc(&c->d_erbase);
+      if (e != cudaSuccess) return fail(SQB200_ENOMEM, std::string("cudaMalloc (error bank): ") + cudaGetErrorString(e));
+      CUDA_OK(cudaMemsetAsync(c->d_erscr, 0, ns * sizeof(unsigned long long), c->stream));
+      CUDA_OK(cudaMemsetAsync(c->d_erbank, sqb::ERR_UNKNOWN, ns, c->stream));
+      CUDA_OK(cudaStreamSynchronize(c->stream));
+      c->er_outer = outer;
+      c->er_total = er_run;
+    }
   }
   auto ins = c->work.emplace(key, w);
   *out = &ins.first->second;
@@ -942,6 +1021,41 @@ int enqueue(const SegLaunch& L, cudaStream_t st) {
   return SQB200_OK;
 }
 
+// Resident CTAs of kernel fn per SM at this block size and dynamic shared memory (cached).
+int resident_ctas(const void* fn, int block, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void*, int, size_t>, int> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 1;
+  std::lock_guard<std::mutex> lock(mu);
+  auto key = std::make_tuple(dev, fn, block, smem);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int n = 0, sms = 0;
+  if (ensure_smem(fn, smem) != SQB200_OK ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, block, smem) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    n = 1; sms = 148;
+  }
+  const int r = std::max(1, n) * std::max(1, sms);
+  cache[key] = r;
+  return r;
+}
+
+// A persistent work-queue launch of segment launch L: a grid of at most one CTA per resident
+// slot of the GPU takes L's (item, pass) units from the zeroed device counter q, in work-list
+// order (heaviest first), instead of one CTA per unit.
+void make_persistent(SegLaunch& L, unsigned long long* q) {
+  const long long units = (long long)L.grid.x * L.grid.y;
+  if (units <= 0 || units > INT_MAX) return;
+  L.a.queue = q;
+  L.a.nqueue = (int)units;
+  L.a.npass = (int)L.grid.y;
+  const int slots = resident_ctas(L.fn, (int)L.block.x, L.smem);
+  L.grid = dim3((unsigned)std::min<long long>(units, slots), 1);
+}
+
 // Segment s of a single-context work list; form < 0 takes the context's choice.
 SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const double* dPA, const double* dPB,
                      int uhf, int form) {
@@ -964,7 +1078,16 @@ SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const dou
   a.mols = c->d_mol;
   a.same_class = K.bra_cls == K.ket_cls;
   L.items = w->d_items + w->first[s];
-  const bool ws = !f32 && c->use_ws && K.ws_r != nullptr;
+  if (c->mp_on && w->d_er) {
+    a.erbank = c->d_erbank;
+    a.erscr = c->d_erscr;
+    a.er_items = w->d_er + w->first[s];
+    a.mpole = c->d_mpole;
+    a.pow15 = c->d_pow15;
+    a.mp_rmax = c->mp_rmax;
+    form = 0;                              // the narrow form carries the multipole mode
+  }
+  const bool ws = !f32 && !c->mp_on && c->use_ws && K.ws_r != nullptr;
   if (!f32) c->ran_ws[kidx] = ws;
   L.smem = (size_t)B.max_nprim * B.stride * (f32 ? sizeof(float) : sizeof(double)) +
            (ws ? (size_t)K.ws_warps * K.ws_nr * 32 * sizeof(double) : 0);
@@ -978,6 +1101,7 @@ SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const dou
   }
   L.grid = dim3(w->count[s], passes);
   L.block = dim3(ws ? 32 * K.ws_warps : cta_threads());
+  if (c->persistent && !ws) make_persistent(L, c->d_queue + v);
   return L;
 }
 
@@ -994,6 +1118,7 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   k_prep<<<grid_for(nn, 256), 256, 0, st>>>(dPA, dPB, c->d_PT, c->d_J, c->d_KA, c->d_KB, nn, uhf, c->d_mol, mv);
   launch_pmax(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM, st);
   CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 8 * sqb::kNumClassKernels, st));
+  if (c->persistent) CUDA_OK(cudaMemsetAsync(c->d_queue, 0, sizeof(unsigned long long) * 2 * sqb::kNumClassKernels, st));
   c->last_launches = 3 + (int)w->kernel.size();
   // segments largest first, each on the least-loaded lane (lane 0 = st, the others are side
   // streams forked off st); per-class profiling keeps every launch on st so that each event
@@ -1034,6 +1159,8 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
     CUDA_OK(cudaEventRecord(c->ev_join[l - 1], c->side[l - 1]));
     CUDA_OK(cudaStreamWaitEvent(st, c->ev_join[l - 1], 0));
   }
+  if (c->mp_on && c->er_total > 0)
+    k_erbank<<<grid_for(c->er_total, 256), 256, 0, st>>>(c->d_erbank, c->d_erscr, c->er_total);
   k_finalize<<<grid_for(nn, 256), 256, 0, st>>>(c->d_J, c->d_KA, c->d_KB, dJT, dKA, dKB, n, uhf);
   CUDA_OK(cudaGetLastError());
   return SQB200_OK;
@@ -1096,6 +1223,50 @@ int time_seg(const SegLaunch& L, cudaStream_t st, int reps, double* ms) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- multipole table (host)
+//
+// genMultipole (reference src/multipole.c:33-86) for every function pair (p, q): the charge
+// q = <p|q> (contracted overlap, set to 0 below 1e-18 in magnitude) and the charge centre, the
+// midpoint of the two function centres moved by dipole/q (the dipole <p|r - mid|q> taken about
+// that midpoint), stored as [q, x, y, z] at 4 (p nbf + q).  Primitive integrals by
+// McMurchie-Davidson: <a|b> = e^{-mu R^2} (pi/p)^{3/2} Ex_0 Ey_0 Ez_0 and
+// <a|x - xc|b> = e^{-mu R^2} (pi/p)^{3/2} (Ex_1 + (Px - xc) Ex_0) Ey_0 Ez_0, summed over the
+// primitives of p (outer) and q (inner) as the reference's GTO_overlap / GTO_moment do.
+void multipole_table(const sqb200_jk* c, std::vector<double>& tab) {
+  const int n = c->nbf;
+  tab.assign((size_t)4 * n * n, 0.0);
+  for (const Shell& A : c->shells)
+    for (const Shell& B : c->shells)
+      for (int f = 0; f < A.nfunc; ++f)
+        for (int g = 0; g < B.nfunc; ++g) {
+          const int la = A.lmn[f][0], ma = A.lmn[f][1], na = A.lmn[f][2];
+          const int lb = B.lmn[g][0], mb = B.lmn[g][1], nb = B.lmn[g][2];
+          const double mx = 0.5 * (A.x + B.x), my = 0.5 * (A.y + B.y), mz = 0.5 * (A.z + B.z);
+          double q = 0.0, dx = 0.0, dy = 0.0, dz = 0.0;
+          for (int k = 0; k < A.nprim; ++k)
+            for (int l = 0; l < B.nprim; ++l) {
+              const double a = A.exps[k], b = B.exps[l], p = a + b, mu = a * b / p;
+              const double Px = (a * A.x + b * B.x) / p, Py = (a * A.y + b * B.y) / p, Pz = (a * A.z + b * B.z) / p;
+              const double R2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
+              double Ex[3][3][5], Ey[3][3][5], Ez[3][3][5];
+              hermite_e(p, Px - A.x, Px - B.x, Ex);
+              hermite_e(p, Py - A.y, Py - B.y, Ey);
+              hermite_e(p, Pz - A.z, Pz - B.z, Ez);
+              const double w = A.coef[k][f] * B.coef[l][g] * exp(-mu * R2) * pow(M_PI / p, 1.5);
+              const double sx = Ex[la][lb][0], sy = Ey[ma][mb][0], sz = Ez[na][nb][0];
+              q += w * sx * sy * sz;
+              dx += w * (Ex[la][lb][1] + (Px - mx) * sx) * sy * sz;
+              dy += w * sx * (Ey[ma][mb][1] + (Py - my) * sy) * sz;
+              dz += w * sx * sy * (Ez[na][nb][1] + (Pz - mz) * sz);
+            }
+          if (fabs(q) < 1e-18) q = 0.0;                  // MULTIPOLE_CHARGE_CUTOFF
+          double x = mx, y = my, z = mz;
+          if (q != 0.0) { x += dx / q; y += dy / q; z += dz / q; }
+          double* o = tab.data() + 4 * ((size_t)(A.first + f) * n + B.first + g);
+          o[0] = q; o[1] = x; o[2] = y; o[3] = z;
+        }
+}
+
 // ---------------------------------------------------------------- C ABI
 
 extern "C" {
@@ -1114,6 +1285,8 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   c->device = device;
   const char* ws_env = getenv("SQB200_WS");
   c->use_ws = !(ws_env && ws_env[0] == '0');
+  const char* pe = getenv("SQB200_PERSISTENT");
+  c->persistent = pe && pe[0] == '1';
   c->ran_ws.assign(sqb::kNumClassKernels, 0);
   c->form.assign(sqb::kNumClassKernels, 0);
   c->ran_form.assign(sqb::kNumClassKernels, 0);
@@ -1138,6 +1311,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
     cv.add(m, nn * sizeof(double));
   cv.add(&c->d_PM, (size_t)c->ns * c->ns * sizeof(double));
   cv.add(&c->d_counters, 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
+  cv.add(&c->d_queue, 2 * sqb::kNumClassKernels * sizeof(unsigned long long));
   cv.add(&c->d_mol, sizeof(sqb::MolRec));
   cudaError_t e = cv.alloc(&c->d_base);
   if (e != cudaSuccess) {
@@ -1176,7 +1350,9 @@ int sqb200_jk_destroy(sqb200_jk* c) {
     cudaEventDestroy(c->ev_join[i]);
   }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-  for (auto& kv : c->work) cudaFree(kv.second.d_items);
+  for (auto& kv : c->work) { cudaFree(kv.second.d_items); cudaFree(kv.second.d_er); }
+  if (c->d_mpbase) cudaFree(c->d_mpbase);
+  if (c->d_erbase) cudaFree(c->d_erbase);
   for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   free_pairs(c);
   cudaFree(c->d_base);
@@ -1352,6 +1528,34 @@ const char* sqb200_jk_class_name(int k) {
 int sqb200_jk_set_precision(sqb200_jk* c, double fp32_below) {
   if (!c || !(fp32_below >= 0.0)) return fail(SQB200_EINVAL, "null context or negative threshold");
   c->fp32_below = fp32_below;
+  return SQB200_OK;
+}
+
+int sqb200_jk_set_persistent(sqb200_jk* c, int enable) {
+  if (!c) return fail(SQB200_EINVAL, "null context");
+  c->persistent = enable != 0;
+  return SQB200_OK;
+}
+
+int sqb200_jk_set_multipole(sqb200_jk* c, int enable, double cache_rmax) {
+  if (!c || (enable && !(cache_rmax >= 0.0))) return fail(SQB200_EINVAL, "null context or negative memory cutoff");
+  CUDA_OK(cudaSetDevice(c->device));
+  if (!enable) {
+    c->mp_on = false;
+    return SQB200_OK;
+  }
+  if (!c->d_mpbase) {
+    std::vector<double> tab, pw(sqb::ERR_MAX - sqb::ERR_MIN + 1);
+    multipole_table(c, tab);
+    for (int e = sqb::ERR_MIN; e <= sqb::ERR_MAX; ++e) pw[e - sqb::ERR_MIN] = pow(1.5, (double)e);
+    Staged sg;
+    sg.put(&c->d_mpole, tab.size() * sizeof(double), tab.data());
+    sg.put(&c->d_pow15, pw.size() * sizeof(double), pw.data());
+    cudaError_t e = sg.upload(&c->d_mpbase, c->stream);
+    if (e != cudaSuccess) return fail(SQB200_ENOMEM, std::string("multipole table: ") + cudaGetErrorString(e));
+  }
+  c->mp_on = true;
+  c->mp_rmax = cache_rmax;
   return SQB200_OK;
 }
 
@@ -1639,6 +1843,8 @@ struct sqb200_batch {
   int *d_shfirst = nullptr, *d_shn = nullptr;
   double *d_PT = nullptr, *d_PM = nullptr, *d_J = nullptr, *d_KA = nullptr, *d_KB = nullptr;
   unsigned long long* d_counters = nullptr;   // 4 per kernel form and spin: [spin][2K][4]
+  unsigned long long* d_queue = nullptr;      // persistent launches: per kernel form and spin [spin][2K]
+  bool persistent = false;
   // work list of the current step: segments per (class kernel form, spin)
   std::vector<int> kernel, spin, first, count;
   std::vector<double> cost;
@@ -1707,7 +1913,7 @@ void free_batch(sqb200_batch* b) {
   if (b->stream) { cudaStreamSynchronize(b->stream); cudaStreamDestroy(b->stream); }
   for (auto& k : b->cls) { cudaFree(k.d_pairs); cudaFree(k.d_prims); cudaFree(k.d_primsf); }
   void* ptrs[] = {b->d_mols, b->d_shfirst, b->d_shn, b->d_PT, b->d_PM, b->d_J, b->d_KA, b->d_KB,
-                  b->d_counters, b->d_items};
+                  b->d_counters, b->d_queue, b->d_items};
   for (void* p : ptrs) cudaFree(p);
   delete b;
 }
@@ -1782,12 +1988,14 @@ extern "C" int sqb200_batch_create(sqb200_batch** out, int nmol, sqb200_jk* cons
   if (e == cudaSuccess) e = cudaMalloc(&b->d_KA, ntot * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_KB, ntot * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 2 * 8 * sqb::kNumClassKernels * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, 2 * 2 * sqb::kNumClassKernels * sizeof(unsigned long long));
   if (e != cudaSuccess) return bail(SQB200_ENOMEM, cudaGetErrorString(e));
   e = h2d(b->d_shfirst, fst.data(), fst.size() * sizeof(int), b->stream);
   if (e == cudaSuccess) e = h2d(b->d_shn, nf.data(), nf.size() * sizeof(int), b->stream);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return bail(SQB200_ECUDA, cudaGetErrorString(e));
   b->form.assign(sqb::kNumClassKernels, 0);
+  b->persistent = mols[0]->persistent;
   b->rec.resize(nmol);
   for (int m = 0; m < nmol; ++m)
     b->rec[m] = sqb::MolRec{b->moff[m], b->pmoff[m], mols[m]->nbf, mols[m]->ns, 0.0, 0.0, 0.0, b->shoff[m], 0};
@@ -1905,6 +2113,7 @@ SegLaunch seg_batch(sqb200_batch* b, size_t s, const double* dPA, const double* 
   L.grid = dim3(b->count[s], passes);
   L.block = dim3(cta_threads());
   add_acc_region(K, fu, L);
+  if (b->persistent) make_persistent(L, b->d_queue + uhf * 2 * K_ + v);
   return L;
 }
 
@@ -1914,6 +2123,12 @@ void batch_prologue(sqb200_batch* b, const double* dPA, const double* dPB, cudaS
                                               nullptr, sqb::MolRec{});
   k_pmax_batch<<<dim3((b->max_ns * b->max_ns + 127) / 128, b->nmol), 128, 0, st>>>(
       dPA, dPB, b->d_PT, b->d_shfirst, b->d_shn, b->d_mols, b->d_PM);
+}
+
+extern "C" int sqb200_batch_set_persistent(sqb200_batch* b, int enable) {
+  if (!b) return fail(SQB200_EINVAL, "null batch");
+  b->persistent = enable != 0;
+  return SQB200_OK;
 }
 
 extern "C" int sqb200_batch_autotune(sqb200_batch* b, const double* dPA, const double* dPB, void* stream) {
@@ -1954,6 +2169,7 @@ extern "C" int sqb200_batch_build_device(sqb200_batch* b, const double* dPA, con
   const int K_ = sqb::kNumClassKernels;
   batch_prologue(b, dPA, dPB, st);
   CUDA_OK(cudaMemsetAsync(b->d_counters, 0, 2 * 8 * K_ * sizeof(unsigned long long), st));
+  if (b->persistent) CUDA_OK(cudaMemsetAsync(b->d_queue, 0, 2 * 2 * K_ * sizeof(unsigned long long), st));
   if (b->nside < 0) {
     int n = 4;
     if (const char* e = getenv("SQB200_STREAMS")) n = std::max(0, std::min(16, atoi(e)));

@@ -19,9 +19,11 @@
  *     uhf_getGMatrix passes and symmetrises them).
  *   - Work is not split over processes: childID 0 builds everything, other children (only
  *     present with -NCPU>1) return zero matrices so uhf_getGMatrix's sum is unchanged.
- * Differences: quartets are evaluated exactly (McMurchie-Davidson in FP64); the reference's
- * monopole approximation for uncached quartets on later visits (src/matrix.c:3945-3949) is not
- * used.  Errors print a message and exit(-1), as the reference does.
+ * Differences: quartets are evaluated exactly (McMurchie-Davidson in FP64) unless
+ * SQB200_MULTIPOLE=1 asks for the reference's monopole approximation of uncached quartets on
+ * later visits (src/matrix.c:3945-3949; sqb200_jk_set_multipole with the memory cutoff of the
+ * first visit), which reproduces the reference's energies under its default 3STEP cutoff
+ * schedule.  Errors print a message and exit(-1), as the reference does.
  * Environment: SQB200_DEVICE selects the CUDA device (default 0); SQB200_FP32_BELOW=<tau>
  * evaluates quartets whose Schwarz product is below tau in FP32 (mixed precision; the
  * reference's SCF passes difference densities, so these errors shrink as SCF converges).
@@ -93,6 +95,9 @@ void GTO_JK_Matrix_Quartet_Parallel(
 		create_context(nBasis, gto, schwarz_basis);
 		int rc = sqb200_jk_mem_cutoff(g_ctx, fixedCutoff, opt->maxMem, &g_memcut);
 		if (rc) die("sqb200_jk_mem_cutoff", rc);
+		const char *mpole = getenv("SQB200_MULTIPOLE");
+		if (mpole && atoi(mpole) == 1 && (rc = sqb200_jk_set_multipole(g_ctx, 1, g_memcut)))
+			die("sqb200_jk_set_multipole", rc);
 	}
 	double dscreen = g_first ? g_memcut : INFINITY;
 	int rc = sqb200_jk_build(g_ctx, PA, PB, opt->restricted, opt->SCFCutoff, fixedCutoff,

@@ -58,6 +58,9 @@ def load_library(path=LIB_PATH):
     L.sqb200_jk_profile_read.argtypes = [vp, _f64p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     L.sqb200_jk_class_name.argtypes = [ctypes.c_int]
     L.sqb200_jk_set_precision.argtypes = [vp, ctypes.c_double]
+    L.sqb200_jk_set_multipole.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+    L.sqb200_jk_set_persistent.argtypes = [vp, ctypes.c_int]
+    L.sqb200_batch_set_persistent.argtypes = [vp, ctypes.c_int]
     L.sqb200_oneint.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
     L.sqb200_peak_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                   ctypes.POINTER(ctypes.c_double)]
@@ -219,6 +222,15 @@ class JKEngine:
         """Quartets with Schwarz product below fp32_below use the FP32 kernel form (0 = FP64)."""
         _check(_lib.sqb200_jk_set_precision(self._ctx, float(fp32_below)))
 
+    def set_multipole(self, enable, cache_rmax=float("inf")):
+        """Reference-parity multipole mode for the following builds (the reference's monopole
+        substitution on later visits of quartets below the memory cutoff cache_rmax)."""
+        _check(_lib.sqb200_jk_set_multipole(self._ctx, int(bool(enable)), float(cache_rmax)))
+
+    def set_persistent(self, enable=True):
+        """Class kernels as persistent work-queue launches (one CTA per resident slot)."""
+        _check(_lib.sqb200_jk_set_persistent(self._ctx, int(bool(enable))))
+
     def oneint(self, charges, coords_bohr):
         """(S, T, V) one-electron matrices for point charges at coords (bohr)."""
         n = self.nbf
@@ -353,6 +365,10 @@ class JKBatch:
     def build_device(self, dPA, dPB, dJT, dKA, dKB, stream=None):
         """Packed device pointers in and out; asynchronous on `stream` (a cudaStream_t handle)."""
         _check(_lib.sqb200_batch_build_device(self._b, dPA, dPB, dJT, dKA, dKB, stream))
+
+    def set_persistent(self, enable=True):
+        """Persistent work-queue launches for this batch's builds."""
+        _check(_lib.sqb200_batch_set_persistent(self._b, int(bool(enable))))
 
     def autotune(self, dPA, dPB, stream=None):
         """Tile autotuner over the batch's current work list (after set_step; synchronous)."""

@@ -16,6 +16,13 @@ job's resident state) -- and frees its slot and memory.
 
 Each job runs exactly the single-job algorithm (scf.SCFJob), so its result is the one it gets
 alone, up to the order of floating-point atomics in the J/K build.
+
+With batched=True (the default) the difference-density J/K builds of all active jobs are one
+batched build (engine.JKBatch: one launch per class kernel over every job's work items, each
+job's own cutoffs, spin and first-visit screen in its molecule record), re-formed whenever a job
+joins or leaves; each job's SCF tail still runs on its own stream.  The server stream waits for
+every job's previous step before it packs the difference densities, and every job's stream waits
+for the build before its tail reads its block of the packed J/K.
 """
 import time
 
@@ -23,6 +30,7 @@ import numpy as np
 
 from . import basis as B
 from . import molecules as M
+from .engine import JKBatch
 from .scf import SCF_MAX, SCFJob, electrons
 
 
@@ -64,13 +72,17 @@ class Server:
     """Continuous-batching SCF server on one device (see the module docstring)."""
 
     def __init__(self, device=0, max_active=32, hbm_budget=None, scf_conv=1e-8, fp32_below=0.0,
-                 max_iter=SCF_MAX, job_factory=None, footprint=footprint_bytes):
+                 max_iter=SCF_MAX, job_factory=None, footprint=footprint_bytes, batched=True):
         """`job_factory(request)` may replace the default SCFJob construction (tests use it to
-        run the scheduler on the CPU with a stand-in J/K engine); `footprint(atoms, basis)`
-        the memory estimate."""
+        run the scheduler on the CPU with a stand-in J/K engine, which also turns the batched
+        builds off); `footprint(atoms, basis)` the memory estimate; `batched` merges the active
+        jobs' J/K builds into one batched build per round."""
         import torch
         self.torch = torch
         self.device = device
+        self.batched = bool(batched) and job_factory is None
+        self._batch = None
+        self._batch_jobs = []
         self.job_factory = job_factory
         self.footprint = footprint
         self.max_active = max_active
@@ -120,9 +132,14 @@ class Server:
                 time.sleep(max(0.0, pending[0]["arrival"] - clock()))
                 continue
             # one SCF step of every active job in flight, then read them back
-            for _r, job, _fp, _ta in active:
-                job.build_jk()
-                job.update_launch()
+            if self.batched:
+                self._batched_builds([job for _r, job, _fp, _ta in active])
+                for _r, job, _fp, _ta in active:
+                    job.update_launch()
+            else:
+                for _r, job, _fp, _ta in active:
+                    job.build_jk()
+                    job.update_launch()
             rounds += 1
             still = []
             for entry in active:
@@ -143,9 +160,65 @@ class Server:
             active = still
         if self.job_factory is None:
             self.torch.cuda.synchronize(self.device)
+        self._drop_batch()
         self.stats = {"makespan": clock(), "peak_active": peak_active, "peak_bytes": peak_used,
                       "rounds": rounds, "budget_bytes": self.hbm_budget}
         return [results[r["id"]] for r in sorted(requests, key=lambda r: r["id"])]
+
+
+    # ------------------------------------------------------------------ batched builds
+    def _drop_batch(self):
+        if self._batch is not None:
+            self._batch.close()
+        self._batch, self._batch_jobs = None, []
+
+    def _batched_builds(self, jobs):
+        """The difference-density J/K of every job in `jobs` as one batched build on the server
+        stream; afterwards each job's dJT/dKA/dKB are views of its blocks of the packed output
+        and its stream waits for the build."""
+        torch = self.torch
+        dev = torch.device("cuda", self.device)
+        if [id(j) for j in jobs] != [id(j) for j in self._batch_jobs]:
+            # re-form on a job joining or leaving: the old packed buffers may still be read by a
+            # job's stream, so everything in flight finishes before they are released
+            torch.cuda.synchronize(dev)
+            self._drop_batch()
+            self._batch = JKBatch([j.eng for j in jobs])
+            self._batch_jobs = list(jobs)
+            if not hasattr(self, "_stream"):
+                self._stream = torch.cuda.Stream(dev)
+            T = self._batch.total
+            f64 = dict(dtype=torch.float64, device=dev)
+            with torch.cuda.stream(self._stream):
+                self._dP = torch.zeros(2 * T, **f64)
+                self._dJT = torch.zeros(T, **f64)
+                self._dKA = torch.zeros(T, **f64)
+                self._dKB = torch.zeros(T, **f64)
+        b, T, st = self._batch, self._batch.total, self._stream
+        # pack every job's difference densities on its own stream, then the build waits for all
+        for m, j in enumerate(jobs):
+            o, n = b.offsets[m], j.n
+            with torch.cuda.stream(j.stream):
+                self._dP[o:o + n * n].view(n, n).copy_(j.PA - j.PA_old)
+                self._dP[T + o:T + o + n * n].view(n, n).copy_(
+                    self._dP[o:o + n * n].view(n, n) if j.restricted else j.PB - j.PB_old)
+                ev = torch.cuda.Event()
+                ev.record(j.stream)
+            st.wait_event(ev)
+        b.set_step([j.restricted for j in jobs], [j.cutoff for j in jobs], [j.cutoff for j in jobs],
+                   [j.rmax_first if j.first else float("inf") for j in jobs])
+        ptr = lambda t, k: t.data_ptr() + 8 * k
+        b.build_device(ptr(self._dP, 0), ptr(self._dP, T), self._dJT.data_ptr(), self._dKA.data_ptr(),
+                       self._dKB.data_ptr(), stream=st.cuda_stream)
+        done = torch.cuda.Event()
+        done.record(st)
+        for m, j in enumerate(jobs):
+            o, n = b.offsets[m], j.n
+            j.dJT = self._dJT[o:o + n * n].view(n, n)
+            j.dKA = self._dKA[o:o + n * n].view(n, n)
+            j.dKB = self._dKB[o:o + n * n].view(n, n)
+            j.first = False
+            j.stream.wait_event(done)
 
 
 def solve_alone(request, device=0, scf_conv=1e-8, fp32_below=0.0):
@@ -158,7 +231,7 @@ def solve_alone(request, device=0, scf_conv=1e-8, fp32_below=0.0):
     e = job.run()
     grad = job.gradient() if (request.get("gradient") and job.converged) else None
     t2 = time.perf_counter()
-    out = (e, job.iters, t2 - t1, t1 - t0, grad)
+    out = (e, job.iters, t2 - t1, t1 - t0, grad, job.n)
     job.close()
     return out
 

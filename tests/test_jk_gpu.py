@@ -163,6 +163,53 @@ def test_c60_full_size_properties():
     assert 30e6 < cnt < 40e6                     # survey: 36.2M survivors for C60/6-31G
 
 
+def c60_fixture():
+    """The C60/6-31G fixture (tests/golden/make_c60_golden.py): the reference's genBasis arrays,
+    Schwarz matrix, its converged SCF density and one fresh reference J/K build from it
+    (direct mode: density screen on every quartet), split over 8 reference processes as
+    uhf_getGMatrix runs it; symmetric matrices come back from their stored upper triangles."""
+    g = golden("c60_631g")
+    n = len(g["nprim"])
+    iu = np.triu_indices(n)
+    for k in ("schwarz", "PA", "JT", "KA"):
+        M = np.zeros((n, n))
+        M[iu] = g.pop(k + "_u")
+        g[k] = M + np.triu(M, 1).T
+    return g
+
+
+def test_c60_fixture_is_consistent():
+    """CPU check of the C60 fixture: 540 functions in the reference's order, the density traces
+    to the 180 occupied orbitals, the outputs are symmetric, J positive and K negative on the
+    diagonal."""
+    g = c60_fixture()
+    b = golden_basis(g)
+    assert b.nbf == 540 and int(g["ncpu"]) == 8
+    S = load_sqb200().checkpoint.overlap_matrix(b, b)
+    assert abs(np.sum(g["PA"] * S) - 180.0) < 1e-6       # tr(PA S) = occupied orbitals
+    assert np.array_equal(g["JT"], g["JT"].T) and np.array_equal(g["KA"], g["KA"].T)
+    assert (np.diag(g["JT"]) > 0).all() and (np.diag(g["KA"]) < 0).all()
+    assert np.allclose(g["schwarz"], g["schwarz"].T)
+
+
+@pytest.mark.gpu
+def test_c60_matches_reference_split_build():
+    """C60/6-31G, 540 functions, element by element against the reference's own build (the sum
+    of its 8 processes' shares), 1e-10 max-abs, from the reference's converged density with
+    its Schwarz matrix; the density screen applies to every quartet as in the reference's
+    direct mode."""
+    g = c60_fixture()
+    eng = _engine(g)
+    JT, KA, KB = eng.build(g["PA"], restricted=True, scf_cutoff=float(g["cutoff"]), dscreen_rmax=float("inf"))
+    errJ = np.abs(JT - g["JT"]).max()
+    errK = np.abs(KA - g["KA"]).max()
+    assert errJ <= TOL and errK <= TOL, (errJ, errK)
+    assert np.array_equal(KB, KA)
+    st = eng.stats()
+    assert 30e6 < st["quartets"] < 40e6
+    eng.close()
+
+
 @pytest.mark.gpu
 def test_mem_cutoff_equals_the_reference_rule():
     """The in-memory cutoff (getMemCutoff, src/matrix.c:3703) is the reference's exact value:
