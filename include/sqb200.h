@@ -267,6 +267,12 @@ int sqb200_jk_mem_cutoff(sqb200_jk *ctx, double fixed_cutoff, int max_mem_mb, do
  * J/K kernels, which run on the FP64 pipe.  (Instrumentation, no reference counterpart.) */
 int sqb200_peak_fma(int device, int fp64_iters, double *fp64_tflops, double *fp32_tflops);
 
+/* F_0..F_mmax(T[i]) for n arguments T[i] >= 0 (mmax <= 8), written to F (n x (mmax + 1)), by
+ * the device Boys function the class kernels use (the role of the reference's fgamma_set,
+ * src/fgamma.c:172-206).  Synchronous; allocates its own device buffers.  (Instrumentation, for
+ * checking the device routine against the reference's.) */
+int sqb200_boys_eval(int device, int mmax, int n, const double *T, double *F);
+
 /* Text of the last error on this thread. */
 const char *sqb200_last_error(void);
 

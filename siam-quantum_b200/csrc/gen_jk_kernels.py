@@ -76,7 +76,10 @@ MIN_BLOCKS = int(os.environ.get("SQB_MINB", "0"))   # __launch_bounds__ min CTAs
 # the same bound for the FP64 narrow-tile form only (its state is smallest, so a register cap
 # spills least there); 0 = none
 MIN_BLOCKS_NARROW = int(os.environ.get("SQB_MINB_NARROW", "0"))
-USE_WS = int(os.environ.get("SQB_WS", "0"))   # also emit warp-specialised multi-pass kernels (measured slower on B200; opt-in)
+USE_WS = int(os.environ.get("SQB_WS", "0"))
+if USE_WS:
+    raise SystemExit("SQB_WS: the warp-specialised form reads primitive records field-contiguously; "
+                     "the pair arrays now store each record's fields kstride apart")   # also emit warp-specialised multi-pass kernels (measured slower on B200; opt-in)
 CTA = 128
 
 
@@ -252,7 +255,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     em("double* __restrict__ KAacc = a.KAacc + mr.moff;")
     em("double* __restrict__ KBacc = a.KBacc + mr.moff;")
     em("const int N = mr.nbf;")
-    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims%s[bp.poff + x];" % (NB, "_f" if F32 else ""))
+    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims%s[bp.poff + (long long)x * bp.kstride];" % (NB, "_f" if F32 else ""))
     em("__syncthreads();")
     em("const int isplit = it.isplit;                 // threads sharing one quartet (bra primitives split)")
     em("const int kl = threadIdx.x / isplit, grp = threadIdx.x - kl * isplit;")
@@ -293,6 +296,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     em("if (ok) {")
     em.ind += 1
     em("const %s* __restrict__ kprim = a.ket_prims%s + kp.poff;" % (RT, "_f" if F32 else ""))
+    em("const int kS = kp.kstride;                   // distance between the fields of one ket record")
     em("const int nbp = %sbp.nprim, nkp = kp.nprim;" % ("mpq ? 0 : " if MP else ""))
     em("nflush = pass == 0 ? (unsigned long long)((nbp - grp + isplit - 1) / isplit) : 0ull;")
     em("const double* __restrict__ PA = a.PA + mr.moff;")
@@ -317,10 +321,10 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
         if ST:
             fields = [0, 1, 2, 3, 4] + [5 + e for (cd, k, e, sg) in kent]
             def stage_code(jexpr, slotexpr):
-                parts = ["const double* __restrict__ src = kprim + (%s) * %d;" % (jexpr, NK),
+                parts = ["const double* __restrict__ src = kprim + (long long)(%s) * %d * kS;" % (jexpr, NK),
                          "const unsigned dst = stg_s + (unsigned)(%s) * %du;" % (slotexpr, nst * 128 * 8)]
                 for fi, f in enumerate(fields):
-                    parts.append('asm volatile("cp.async.ca.shared.global [%%0], [%%1], 8;" :: "r"(dst + %du), "l"(src + %d) : "memory");' % (fi * 128 * 8, f))
+                    parts.append('asm volatile("cp.async.ca.shared.global [%%0], [%%1], 8;" :: "r"(dst + %du), "l"(src + %d * kS) : "memory");' % (fi * 128 * 8, f))
                 return "{ " + " ".join(parts) + " }"
             # the first record of the sequence (i, j) = (grp, 0), (grp, 1), ..., (grp + isplit, 0), ...
             em("int slot = 0;")
@@ -339,9 +343,9 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
             em("double nq = 0.0, nQx = 0.0, nQy = 0.0, nQz = 0.0, nkq = 0.0;")
             for (cd, k, e, sg) in kent:
                 em("%s nek%d_%d = 0;" % (RT, cd, k))
-            em("if (nkp > 0) { nq = kprim[0]; nQx = kprim[1]; nQy = kprim[2]; nQz = kprim[3]; nkq = kprim[4];")
+            em("if (nkp > 0) { nq = kprim[0]; nQx = kprim[kS]; nQy = kprim[2 * kS]; nQz = kprim[3 * kS]; nkq = kprim[4 * kS];")
             for (cd, k, e, sg) in kent:
-                em("  nek%d_%d = %skprim[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
+                em("  nek%d_%d = %skprim[%d * kS];" % (cd, k, "-" if sg < 0 else "", 5 + e))
             em("}")
         em("for (int j = 0; j < nkp; ++j) {")
         em.ind += 1
@@ -361,20 +365,20 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
             em("const double q = nq, Qx = nQx, Qy = nQy, Qz = nQz, kq = nkq;")
             for (cd, k, e, sg) in kent:
                 em("const %s ek%d_%d = nek%d_%d;" % (RT, cd, k, cd, k))
-            em("if (j + 1 < nkp) { const %s* __restrict__ kn = kprim + (j + 1) * %d;" % (RT, NK))
-            em("  nq = kn[0]; nQx = kn[1]; nQy = kn[2]; nQz = kn[3]; nkq = kn[4];")
+            em("if (j + 1 < nkp) { const %s* __restrict__ kn = kprim + (long long)(j + 1) * %d * kS;" % (RT, NK))
+            em("  nq = kn[0]; nQx = kn[kS]; nQy = kn[2 * kS]; nQz = kn[3 * kS]; nkq = kn[4 * kS];")
             for (cd, k, e, sg) in kent:
-                em("  nek%d_%d = %skn[%d];" % (cd, k, "-" if sg < 0 else "", 5 + e))
+                em("  nek%d_%d = %skn[%d * kS];" % (cd, k, "-" if sg < 0 else "", 5 + e))
             em("}")
             em("const double pq = p + q;")
             em("const double rs = rsqrt(pq);")
             em("if (TWO_PI_2_5 * kpb * kq * rs < PRIM_CUTOFF) continue;")
         else:
-            em("const %s* __restrict__ kj = kprim + j * %d;" % (RT, NK))
+            em("const %s* __restrict__ kj = kprim + (long long)j * %d * kS;" % (RT, NK))
             em("const double q = kj[0];")
             em("const double pq = p + q;")
             em("const double rs = rsqrt(pq);")
-            em("if (TWO_PI_2_5 * kpb * kj[4] * rs < PRIM_CUTOFF) continue;")
+            em("if (TWO_PI_2_5 * kpb * kj[4 * kS] * rs < PRIM_CUTOFF) continue;")
         if bi == 0:
             em("++nprimq;")   # counted by the pass-0 CTAs only
         em("const double alpha = p * q * (rs * rs);")
@@ -383,7 +387,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
         elif PREFETCH:
             em("const double X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;")
         else:
-            em("const double X = Px - kj[1], Y = Py - kj[2], Z = Pz - kj[3];")
+            em("const double X = Px - kj[kS], Y = Py - kj[2 * kS], Z = Pz - kj[3 * kS];")
         em("const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));")
         need = set()
         for cd in blk:
@@ -409,7 +413,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
                 em("const %s ek%d_%d = %ssv[%d];" % (RT, cd, k, "-" if sg < 0 else "", (5 + fi) * 128))
         elif not PREFETCH:
             for (cd, k, e, sg) in kent:
-                em("const %s ek%d_%d = %skj[%d];" % (RT, cd, k, "-" if sg < 0 else "", 5 + e))
+                em("const %s ek%d_%d = %skj[%d * kS];" % (RT, cd, k, "-" if sg < 0 else "", 5 + e))
         # consumers of each R value: (cd, k, h) with h + (tau nu phi) = R index
         cons = {}
         for cd in blk:
@@ -560,7 +564,7 @@ def gen_class_swap(bra, ket, spin, state_max):
     em("double* __restrict__ KAacc = a.KAacc + mr.moff;")
     em("double* __restrict__ KBacc = a.KBacc + mr.moff;")
     em("const int N = mr.nbf;")
-    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
+    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + (long long)x * bp.kstride];" % NB)
     em("__syncthreads();")
     em("const int isplit = it.isplit;                 // threads sharing one quartet (ket primitives split)")
     em("const int kl = threadIdx.x / isplit, grp = threadIdx.x - kl * isplit;")
@@ -589,6 +593,7 @@ def gen_class_swap(bra, ket, spin, state_max):
     em("if (ok) {")
     em.ind += 1
     em("const double* __restrict__ kprim = a.ket_prims + kp.poff;")
+    em("const int kS = kp.kstride;                   // distance between the fields of one ket record")
     em("const int nbp = bp.nprim, nkp = kp.nprim;")
     em("nflush = pass == 0 ? (unsigned long long)((nkp - grp + isplit - 1) / isplit) : 0ull;")
     em("const double* __restrict__ PA = a.PA + mr.moff;")
@@ -608,8 +613,8 @@ def gen_class_swap(bra, ket, spin, state_max):
                     em("double o%d_%d = 0;" % (ab, cd))
         em("for (int j = grp; j < nkp; j += isplit) {")
         em.ind += 1
-        em("const double* __restrict__ kj = kprim + j * %d;" % NK)
-        em("const double q = kj[0], Qx = kj[1], Qy = kj[2], Qz = kj[3], kq = kj[4];")
+        em("const double* __restrict__ kj = kprim + (long long)j * %d * kS;" % NK)
+        em("const double q = kj[0], Qx = kj[kS], Qy = kj[2 * kS], Qz = kj[3 * kS], kq = kj[4 * kS];")
         for ab in blk:
             for k in Hk:
                 em("double g%d_%d = 0;" % (ab, kidx[k]))
@@ -665,7 +670,7 @@ def gen_class_swap(bra, ket, spin, state_max):
                 ks = list(enumerate(nz(fk[cd])))
                 em("{")
                 for e, k in ks:
-                    em("  const double ek%d = %skj[%d];" % (e, "-" if sum(k) % 2 else "", 5 + offk[cd] + e))
+                    em("  const double ek%d = %skj[%d * kS];" % (e, "-" if sum(k) % 2 else "", 5 + offk[cd] + e))
                 for ab in blk:
                     em("  { double t = %s;" % slot(ab, cd))
                     for e, k in ks:
@@ -677,7 +682,7 @@ def gen_class_swap(bra, ket, spin, state_max):
             for cd in range(ncd):
                 for e, k in enumerate(nz(fk[cd])):
                     sg = "-" if sum(k) % 2 else ""
-                    em("{ const double ek = %skj[%d];" % (sg, 5 + offk[cd] + e))
+                    em("{ const double ek = %skj[%d * kS];" % (sg, 5 + offk[cd] + e))
                     for ab in blk:
                         em("  o%d_%d = fma(ek, g%d_%d, o%d_%d);" % (ab, cd, ab, kidx[k], ab, cd))
                         ff += 2
@@ -855,7 +860,7 @@ def gen_class_ws(bra, ket, spin):
     em("double* __restrict__ KAacc = a.KAacc + mr.moff;")
     em("double* __restrict__ KBacc = a.KBacc + mr.moff;")
     em("const int N = mr.nbf;")
-    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + x];" % NB)
+    em("for (int x = threadIdx.x; x < bp.nprim * %d; x += blockDim.x) sbra[x] = a.bra_prims[bp.poff + (long long)x * bp.kstride];" % NB)
     em("__syncthreads();")
     em("const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;")
     em("bool ok = lane < it.cnt;")

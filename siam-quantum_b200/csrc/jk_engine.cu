@@ -1223,6 +1223,24 @@ int time_seg(const SegLaunch& L, cudaStream_t st, int reps, double* ms) {
 
 }  // namespace
 
+// ---------------------------------------------------------------- Boys function check
+
+// F_0..F_M(T[i]) by the class kernels' own device routine sqb::boys<M>.
+template <int M>
+__global__ void k_boys_eval(const double* __restrict__ T, int n, const double* __restrict__ tab,
+                            double* __restrict__ F) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double f[M + 1];
+  sqb::boys<M>(T[i], tab, f);
+  for (int m = 0; m <= M; ++m) F[(size_t)i * (M + 1) + m] = f[m];
+}
+
+template <int M>
+void launch_boys(const double* T, int n, const double* tab, double* F) {
+  k_boys_eval<M><<<(n + 127) / 128, 128>>>(T, n, tab, F);
+}
+
 // ---------------------------------------------------------------- multipole table (host)
 //
 // genMultipole (reference src/multipole.c:33-86) for every function pair (p, q): the charge
@@ -1528,6 +1546,40 @@ const char* sqb200_jk_class_name(int k) {
 int sqb200_jk_set_precision(sqb200_jk* c, double fp32_below) {
   if (!c || !(fp32_below >= 0.0)) return fail(SQB200_EINVAL, "null context or negative threshold");
   c->fp32_below = fp32_below;
+  return SQB200_OK;
+}
+
+int sqb200_boys_eval(int device, int mmax, int n, const double* T, double* F) {
+  if (!T || !F || n <= 0 || mmax < 0 || mmax > BOYS_MMAX)
+    return fail(SQB200_EINVAL, "sqb200_boys_eval: null array, n <= 0 or mmax outside 0..8");
+  for (int i = 0; i < n; ++i)
+    if (!(T[i] >= 0.0)) return fail(SQB200_EINVAL, "sqb200_boys_eval: T must be >= 0");
+  CUDA_OK(cudaSetDevice(device));
+  const std::vector<double> tab = make_boys_table();
+  double *dT = nullptr, *dF = nullptr, *dtab = nullptr;
+  const size_t nf = (size_t)n * (mmax + 1);
+  cudaError_t e = cudaMalloc(&dT, n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dF, nf * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dtab, tab.size() * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(dT, T, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dtab, tab.data(), tab.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    switch (mmax) {
+      case 0: launch_boys<0>(dT, n, dtab, dF); break;
+      case 1: launch_boys<1>(dT, n, dtab, dF); break;
+      case 2: launch_boys<2>(dT, n, dtab, dF); break;
+      case 3: launch_boys<3>(dT, n, dtab, dF); break;
+      case 4: launch_boys<4>(dT, n, dtab, dF); break;
+      case 5: launch_boys<5>(dT, n, dtab, dF); break;
+      case 6: launch_boys<6>(dT, n, dtab, dF); break;
+      case 7: launch_boys<7>(dT, n, dtab, dF); break;
+      default: launch_boys<8>(dT, n, dtab, dF); break;
+    }
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(F, dF, nf * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(dT); cudaFree(dF); cudaFree(dtab);
+  if (e != cudaSuccess) return fail(SQB200_ECUDA, std::string("sqb200_boys_eval: ") + cudaGetErrorString(e));
   return SQB200_OK;
 }
 

@@ -28,7 +28,8 @@ EXPORTS = ["sqb200_jk_create", "sqb200_jk_destroy", "sqb200_jk_build", "sqb200_j
            "sqb200_batch_autotune", "sqb200_jk_autotune", "sqb200_jk_tiles", "sqb200_jk_set_tiles",
            "sqb200_syev_batched", "sqb200_gradient", "sqb200_gradient_terms",
            "sqb200_segdots_create", "sqb200_segdots_run", "sqb200_segdots_destroy",
-           "sqb200_last_error"]
+           "sqb200_jk_set_multipole", "sqb200_jk_set_persistent", "sqb200_batch_set_persistent",
+           "sqb200_boys_eval", "sqb200_last_error"]
 
 
 class SQB200Error(RuntimeError):
@@ -60,6 +61,7 @@ def load_library(path=LIB_PATH):
     L.sqb200_jk_set_precision.argtypes = [vp, ctypes.c_double]
     L.sqb200_jk_set_multipole.argtypes = [vp, ctypes.c_int, ctypes.c_double]
     L.sqb200_jk_set_persistent.argtypes = [vp, ctypes.c_int]
+    L.sqb200_boys_eval.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p, _f64p]
     L.sqb200_batch_set_persistent.argtypes = [vp, ctypes.c_int]
     L.sqb200_oneint.argtypes = [vp, ctypes.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
     L.sqb200_peak_fma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
@@ -390,3 +392,12 @@ class JKBatch:
             self.close()
         except Exception:
             pass
+
+
+def boys_eval(mmax, T, device=0):
+    """F_0..F_mmax at each T by the device Boys function of the class kernels (len(T) x (mmax+1))."""
+    L = load_library()
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    F = np.empty((len(T), mmax + 1))
+    _check(L.sqb200_boys_eval(int(device), int(mmax), len(T), T, F))
+    return F

@@ -33,13 +33,16 @@ def _requests(sqb):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("batched", [True, False])
 @pytest.mark.parametrize("two_slots_by_memory", [False, True])
-def test_served_results_equal_alone(two_slots_by_memory):
+def test_served_results_equal_alone(two_slots_by_memory, batched):
+    """batched: the active jobs' J/K in one batched build per round (re-formed as jobs come and
+    go); otherwise one build per job on its own stream."""
     sqb = load_sqb200()
     reqs = _requests(sqb)
     fps = [sqb.serve.footprint_bytes(r["atoms"], r["basis"]) for r in reqs]
     budget = max(fps) + min(fps) if two_slots_by_memory else None
-    srv = sqb.serve.Server(max_active=8, hbm_budget=budget)
+    srv = sqb.serve.Server(max_active=8, hbm_budget=budget, batched=batched)
     res = srv.run(reqs, realtime=True)
     alone = [sqb.serve.solve_alone(r) for r in reqs]
     if two_slots_by_memory:
@@ -57,7 +60,7 @@ def test_served_results_equal_alone(two_slots_by_memory):
         assert abs(o["iters"] - a[1]) <= 1
         if r.get("gradient"):
             assert np.abs(o["gradient"] - a[4]).max() <= 1e-8
-    with open(results_path("serve_vs_alone_%d.json" % two_slots_by_memory), "w") as f:
+    with open(results_path("serve_vs_alone_%d_%d.json" % (two_slots_by_memory, batched)), "w") as f:
         json.dump({"jobs": out, "stats": srv.stats}, f)
     # the golden molecules also reach the reference's energies
     for c, o in zip(GOLDEN_CASES, res):
