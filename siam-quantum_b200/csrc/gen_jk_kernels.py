@@ -50,6 +50,9 @@ PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
 # bra/ket orientation: the larger pair (by functions, then L) is the bra
 PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
 STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out accumulators per pass
+# the mixed (FP32) form: floats of G + out per pass -- one register each, so twice the values of
+# the narrow FP64 form in the same registers
+STATE_MAX_F32 = int(os.environ.get("SQB_STATE_MAX_F32", "128"))
 # the wide tile: a second FP64 form of every class whose passes it merges (fewer passes, each
 # re-deriving the Boys function and R for more ket functions, at more registers); which form a
 # class runs is chosen by measurement (sqb200_jk_autotune)
@@ -219,7 +222,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     nc, nd = len(COMP[ket[0]]), len(COMP[ket[1]])
     NB = 5 + len(layb)
     NK = 5 + len(layk)
-    per = ket_per_pass(bra, ket, STATE_MAX if state_max is None else state_max, smem_o)
+    per = ket_per_pass(bra, ket, (STATE_MAX_F32 if F32 else STATE_MAX) if state_max is None else state_max, smem_o)
     blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
     name = "jk_%s_%s_%s%s%s" % (bra, ket, spin, "_f32" if F32 else "", suffix)
     SO = smem_o and not F32
@@ -333,7 +336,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
         em("for (int i = grp; i < nbp; i += isplit) {")
         em.ind += 1
         em("const %s* __restrict__ bi = sbra + i * %d;" % (RT, NB))
-        em("const double p = bi[0], Px = bi[1], Py = bi[2], Pz = bi[3], kpb = bi[4];")
+        em("const %s p = bi[0], Px = bi[1], Py = bi[2], Pz = bi[3], kpb = bi[4];" % RT)
         for cd in blk:
             for h in Hb:
                 em("%s g%d_%d = 0;" % (RT, cd, hidx[h]))
@@ -373,6 +376,14 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
             em("const double pq = p + q;")
             em("const double rs = rsqrt(pq);")
             em("if (TWO_PI_2_5 * kpb * kq * rs < PRIM_CUTOFF) continue;")
+        elif F32:
+            # the mixed form: every step in FP32 (records, set-up, Boys function, recursion,
+            # contraction); only the digestion adds into the FP64 accumulators
+            em("const float* __restrict__ kj = kprim + (long long)j * %d * kS;" % NK)
+            em("const float q = kj[0];")
+            em("const float pq = p + q;")
+            em("const float rs = rsqrtf(pq);")
+            em("if (TWO_PI_2_5F * kpb * kj[4 * kS] * rs < PRIM_CUTOFF_F) continue;")
         else:
             em("const %s* __restrict__ kj = kprim + (long long)j * %d * kS;" % (RT, NK))
             em("const double q = kj[0];")
@@ -381,31 +392,38 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
             em("if (TWO_PI_2_5 * kpb * kj[4 * kS] * rs < PRIM_CUTOFF) continue;")
         if bi == 0:
             em("++nprimq;")   # counted by the pass-0 CTAs only
-        em("const double alpha = p * q * (rs * rs);")
+        em("const %s alpha = p * q * (rs * rs);" % RT)
         if ST:
             em("const double X = Px - sv[%d], Y = Py - sv[%d], Z = Pz - sv[%d];" % (128, 256, 384))
         elif PREFETCH:
             em("const double X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;")
         else:
-            em("const double X = Px - kj[kS], Y = Py - kj[2 * kS], Z = Pz - kj[3 * kS];")
-        em("const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));")
+            em("const %s X = Px - kj[kS], Y = Py - kj[2 * kS], Z = Pz - kj[3 * kS];" % RT)
+        em("const %s T = alpha * %s(X, X, %s(Y, Y, Z * Z));" % (RT, FMA, FMA))
         need = set()
         for cd in blk:
             for (tau, nu, phi) in nz(fk[cd]):
                 for h in Hb:
                     need.add((h[0] + tau, h[1] + nu, h[2] + phi))
         Lp = max(sum(x) for x in need)          # highest Hermite order this pass needs
-        em("double F[%d];" % (Lp + 1))
-        em("sqb::boys<%d>(T, a.boys_tab, F);" % Lp)
-        em("const double s0 = TWO_PI_2_5 * rs;")
-        em("const double m2a = -2.0 * alpha;")
-        em("double w = s0;")
+        if F32:
+            em("float F[%d];" % (Lp + 1))
+            em("sqb::boysf<%d>(T, a.boys_tab_f, F);" % Lp)
+            em("const float s0 = TWO_PI_2_5F * rs;")
+            em("const float m2a = -2.0f * alpha;")
+            em("float w = s0;")
+        else:
+            em("double F[%d];" % (Lp + 1))
+            em("sqb::boys<%d>(T, a.boys_tab, F);" % Lp)
+            em("const double s0 = TWO_PI_2_5 * rs;")
+            em("const double m2a = -2.0 * alpha;")
+            em("double w = s0;")
         pf = 9 + 2 + 3 + 5 + boys_flops(Lp) + 2  # setup: pq, alpha, XYZ diff, T, s0, m2a
         for n in range(Lp + 1):
             if n > 0:
                 em("w *= m2a;")
                 pf += 1
-            em("const %s b%d = %s(w * F[%d]);" % (RT, n, "(float)" if F32 else "", n))
+            em("const %s b%d = w * F[%d];" % (RT, n, n))
             pf += 1
         # ket E coefficients of this block, signed by (-1)^(tau+nu+phi)
         if ST:
@@ -1049,41 +1067,46 @@ def main():
     os.makedirs(outdir, exist_ok=True)
     metas = []
     files = []
+    head = ['// generated by gen_jk_kernels.py -- do not edit', '#include "../jk_common.cuh"', '']
+
+    def emit(src, meta):
+        # one kernel per file: the largest classes' kernels take ptxas minutes each, and
+        # separate files compile in parallel
+        fn = "%s.cu" % meta["name"]
+        write_if_changed(os.path.join(outdir, fn), "\n".join(head + [src]))
+        files.append(fn)
+
     for bra, ket in quartet_classes():
-        src = ['// generated by gen_jk_kernels.py -- do not edit', '#include "../jk_common.cuh"', '']
         for spin in ("R", "U"):
             s, m = gen_class(bra, ket, spin)
-            src.append(s)
+            emit(s, m)
             m["ws"] = None
             if USE_WS and ws_plan(bra, ket) is not None:
                 s2, m2 = gen_class_ws(bra, ket, spin)
-                src.append(s2)
+                emit(s2, m2)
                 m["ws"] = m2
             m["wide"] = None
             if WIDE_SMEM:
                 fb_, _, _ = etable(bra)
                 if len(fb_) * ket_per_pass(bra, ket, 0, True) >= 8:
                     s4, m4 = gen_class(bra, ket, spin, "D", None, "_w", smem_o=True)
-                    src.append(s4)
+                    emit(s4, m4)
                     m["wide"] = m4
             elif n_passes(bra, ket, STATE_MAX_WIDE) < n_passes(bra, ket, STATE_MAX):
                 s4, m4 = gen_class(bra, ket, spin, "D", STATE_MAX_WIDE, "_w", stage=bool(STAGE_WIDE))
-                src.append(s4)
+                emit(s4, m4)
                 m["wide"] = m4
             m["swap"] = None
             if SWAP and swap_worthwhile(bra, ket):
                 s5, m5 = gen_class_swap(bra, ket, spin, STATE_MAX_SWAP)
-                src.append(s5)
+                emit(s5, m5)
                 m["swap"] = m5
             m["f32"] = None
             if pair_L(bra) + pair_L(ket) <= F32_MAX_L:
                 s3, m3 = gen_class(bra, ket, spin, "F")
-                src.append(s3)
+                emit(s3, m3)
                 m["f32"] = m3
             metas.append(m)
-        fn = "jk_%s_%s.cu" % (bra, ket)
-        write_if_changed(os.path.join(outdir, fn), "\n".join(src))
-        files.append(fn)
     # registry
     reg = ['// generated by gen_jk_kernels.py -- do not edit', '#include "../jk_common.cuh"',
            '#include "../jk_registry.h"', '']
@@ -1147,6 +1170,10 @@ def main():
     fj.update({m["wide"]["name"]: m["wide"]["flops"] for m in metas if m["wide"]})
     fj.update({m["swap"]["name"]: m["swap"]["flops"] for m in metas if m["swap"]})
     write_if_changed(os.path.join(outdir, "jk_flops.json"), json.dumps(fj, indent=0))
+    # sources of an earlier layout that this run did not write
+    for fn in os.listdir(outdir):
+        if fn.endswith(".cu") and fn not in files:
+            os.remove(os.path.join(outdir, fn))
     write_if_changed(os.path.join(outdir, "files.txt"), "\n".join(files) + "\n")
     print("generated %d kernels in %d files" % (len(metas), len(files)))
 

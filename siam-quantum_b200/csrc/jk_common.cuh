@@ -29,7 +29,10 @@ struct PairRec {
   int P, Q;        // sorted shell indices
   int fP, fQ;      // first basis function of each shell
   int nprim;       // primitive pairs
-  int poff;        // offset (doubles) of the first primitive record in the class array
+  int poff;        // offset (elements) of field 0 of its first primitive record in the class array
+  int kstride;     // elements between consecutive fields of one record: field f of primitive
+                   // record j sits at poff + (j * fields + f) * kstride
+  int pad_;
   double schwarz;  // max over the block of the basis-level Schwarz matrix
 };
 

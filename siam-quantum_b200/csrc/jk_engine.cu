@@ -440,11 +440,12 @@ __global__ void k_schwarz(const sqb::PairRec* __restrict__ pairs, const double* 
   double acc = 0.0;
   double Ra[165], Rb[165], F[9];
   for (int i = 0; i < rec.nprim; ++i) {
-    const double* pi = prims + rec.poff + i * stride;
+    const int ks = rec.kstride;
+    const double* pi = prims + rec.poff + (long long)i * stride * ks;
     for (int j = 0; j < rec.nprim; ++j) {
-      const double* pj = prims + rec.poff + j * stride;
+      const double* pj = prims + rec.poff + (long long)j * stride * ks;
       const double p = pi[0], q = pj[0], pq = p + q, rs = rsqrt(pq), alpha = p * q * (rs * rs);
-      const double X = pi[1] - pj[1], Y = pi[2] - pj[2], Z = pi[3] - pj[3];
+      const double X = pi[ks] - pj[ks], Y = pi[2 * ks] - pj[2 * ks], Z = pi[3 * ks] - pj[3 * ks];
       const double T = alpha * (X * X + Y * Y + Z * Z);
       sqb::boys<8>(T, tab, F);
       // R^{(n)} from n = L down to 0
@@ -475,13 +476,13 @@ __global__ void k_schwarz(const sqb::PairRec* __restrict__ pairs, const double* 
       for (int t = 0; t <= sx; ++t)
         for (int u = 0; u <= sy; ++u)
           for (int v = 0; v <= sz; ++v, ++ka) {
-            const double ea = pi[5 + eo + ka];
+            const double ea = pi[(5 + eo + ka) * ks];
             int kb = 0;
             double s = 0.0;
             for (int tt = 0; tt <= sx; ++tt)
               for (int uu = 0; uu <= sy; ++uu)
                 for (int vv = 0; vv <= sz; ++vv, ++kb) {
-                  const double e = pj[5 + eo + kb];
+                  const double e = pj[(5 + eo + kb) * ks];
                   s += (((tt + uu + vv) & 1) ? -e : e) * cur[tetra(t + tt, u + uu, v + vv)];
                 }
             acc += ea * s;
@@ -627,6 +628,14 @@ void build_pairs(sqb200_jk* c) {
       const int k = pair_class_of(sh[P].type, sh[Q].type);
       lists[k].push_back({sch(P, Q), P, Q, sh[P].nprim * sh[Q].nprim});
     }
+  // Layout of a class's primitive records: inside each run of pairs with one primitive count
+  // (a sub-list, S pairs), field f of record j of the run's pair l is element
+  // run_base + (j * stride + f) * S + l -- consecutive pairs side by side, so the lanes of a
+  // warp, which hold consecutive ket pairs of one sub-list, read one field of their records in
+  // coalesced loads (PairRec::poff = run_base + l, kstride = S).  SQB200_AOS=1 keeps each
+  // record's fields contiguous instead (kstride 1), for comparison.
+  const char* aos_env = getenv("SQB200_AOS");
+  const bool aos = aos_env && aos_env[0] == '1';
   for (int k = 0; k < sqb::kNumPairClasses; ++k) {
     PairClass& pc = c->cls[k];
     std::stable_sort(lists[k].begin(), lists[k].end(),
@@ -648,6 +657,8 @@ void build_pairs(sqb200_jk* c) {
       rec.P = t.P; rec.Q = t.Q; rec.fP = A.first; rec.fQ = B.first;
       rec.nprim = A.nprim * B.nprim;
       rec.poff = (int)pc.prims.size();
+      rec.kstride = 1;
+      rec.pad_ = 0;
       rec.schwarz = t.s;
       pc.max_nprim = std::max(pc.max_nprim, rec.nprim);
       const double ab2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
@@ -677,6 +688,22 @@ void build_pairs(sqb200_jk* c) {
             }
         }
       pc.pairs.push_back(rec);
+    }
+    if (!aos) {
+      // records were appended contiguously (pair-major); transpose every sub-list run
+      std::vector<double> soa(pc.prims.size());
+      for (size_t r = 0; r + 1 < pc.sub.size(); ++r) {
+        const int l0 = pc.sub[r], l1 = pc.sub[r + 1], S = l1 - l0;
+        const size_t base = (size_t)pc.pairs[l0].poff;
+        const size_t per = (size_t)pc.pairs[l0].nprim * pc.stride;   // elements per pair
+        for (int l = 0; l < S; ++l) {
+          const double* src = pc.prims.data() + base + (size_t)l * per;
+          for (size_t e = 0; e < per; ++e) soa[base + e * S + l] = src[e];
+          pc.pairs[l0 + l].poff = (int)(base + l);
+          pc.pairs[l0 + l].kstride = S;
+        }
+      }
+      pc.prims.swap(soa);
     }
   }
 }
@@ -1054,6 +1081,9 @@ void make_persistent(SegLaunch& L, unsigned long long* q) {
   L.a.npass = (int)L.grid.y;
   const int slots = resident_ctas(L.fn, (int)L.block.x, L.smem);
   L.grid = dim3((unsigned)std::min<long long>(units, slots), 1);
+  static const bool trace = getenv("SQB200_TRACE_PERSISTENT") != nullptr;
+  if (trace) fprintf(stderr, "persistent launch %p: %lld units, %d resident CTAs, grid %u x %u threads\n", L.fn, units,
+                     slots, L.grid.x, L.block.x);
 }
 
 // Segment s of a single-context work list; form < 0 takes the context's choice.
