@@ -50,9 +50,9 @@ PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
 # bra/ket orientation: the larger pair (by functions, then L) is the bra
 PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
 STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out accumulators per pass
-# the mixed (FP32) form: floats of G + out per pass -- one register each, so twice the values of
-# the narrow FP64 form in the same registers
-STATE_MAX_F32 = int(os.environ.get("SQB_STATE_MAX_F32", "128"))
+# the mixed (FP32) form: floats of G + out per pass (a float takes one register; measured on
+# LL|LL: 64 floats -> 8 passes at 188 registers, 96 -> 6 passes at 242, 128 -> spills)
+STATE_MAX_F32 = int(os.environ.get("SQB_STATE_MAX_F32", "96"))
 # the wide tile: a second FP64 form of every class whose passes it merges (fewer passes, each
 # re-deriving the Boys function and R for more ket functions, at more registers); which form a
 # class runs is chosen by measurement (sqb200_jk_autotune)
@@ -509,8 +509,11 @@ def persistent_body(lines):
     """Wrap a class kernel's body in the work loop of the persistent launch.  A work unit is one
     (work item, pass) pair.  With a.queue null the CTA runs the unit (blockIdx.x, blockIdx.y)
     and stops (one CTA per unit); otherwise a grid of about one CTA per resident slot takes
-    units from the device counter a.queue -- unit q is item q / npass, pass q % npass, heaviest
-    items first as the work list orders them -- until the a.nqueue units are taken."""
+    units from the device counter a.queue until the a.nqueue units are taken.  Unit q is item
+    q % nitems of pass q / nitems -- the order in which the hardware hands out the CTAs of a
+    (items x passes) grid, heaviest items first in each pass -- so that the CTAs running at one
+    time work on different items: the passes of one item digest into the same exchange
+    elements, and running them side by side would queue their atomics on the same addresses."""
     body = [l.replace("blockIdx.x", "qi_").replace("blockIdx.y", "qp_") for l in lines]
     out = ["  __shared__ int q_next;",
            "  const bool persistent = a.queue != nullptr;",
@@ -522,8 +525,9 @@ def persistent_body(lines):
            "      __syncthreads();",
            "      const int q = q_next;",
            "      if (q >= a.nqueue) break;",
-           "      qi_ = q / a.npass;",
-           "      qp_ = q - qi_ * a.npass;",
+           "      const int nitems = a.nqueue / a.npass;",
+           "      qp_ = q / nitems;",
+           "      qi_ = q - qp_ * nitems;",
            "    } else {",
            "      if (round > 0) break;",
            "      qi_ = blockIdx.x;",

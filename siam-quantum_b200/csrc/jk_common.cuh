@@ -21,6 +21,8 @@
 
 #define TWO_PI_2_5  34.986836655249725     // 2 pi^(5/2)
 #define PRIM_CUTOFF 1.0e-15                // reference src/int.h:19
+#define TWO_PI_2_5F 34.986836655249725f    // the same in FP32 (mixed-precision forms)
+#define PRIM_CUTOFF_F 1.0e-15f
 
 namespace sqb {
 
@@ -68,6 +70,7 @@ struct JKArgs {
   double* KAacc;               // per molecule nbf x nbf, K[PA] = KAacc + KAacc^T
   double* KBacc;
   const double* boys_tab;      // BOYS_NGRID x BOYS_NCOL
+  const float* boys_tab_f;     // the same table rounded to FP32 (mixed-precision forms)
   unsigned long long* counters;// [0] quartets computed, [1] primitive quartets evaluated,
                                // [2] bra-primitive flushes, [3] digestions
   const MolRec* mols;          // per-molecule offsets, sizes and cutoffs (WorkItem::mol)
@@ -138,6 +141,37 @@ __device__ __forceinline__ void boys(double T, const double* __restrict__ tab, d
       const double h = 0.5 * it;
 #pragma unroll
       for (int m = 0; m < M; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * h;
+    }
+  }
+}
+
+// F_0..F_M at T in FP32, for the mixed-precision forms (quartets whose Schwarz bound is below
+// the FP32 threshold): the scheme of boys<M> with the FP32 table and 6 Taylor terms
+// (|d| <= BOYS_H/2: the next term is below 2e-11 of F_M, under FP32 rounding).
+template <int M>
+__device__ __forceinline__ void boysf(float T, const float* __restrict__ tab, float* F) {
+  if (T < (float)BOYS_TMAX) {
+    const int g = __float2int_rn(T * (float)BOYS_INV_H);
+    const float d = T - g * (float)BOYS_H;
+    const float* row = tab + g * BOYS_NCOL + M;
+    float s = row[5];
+#pragma unroll
+    for (int k = 4; k >= 0; --k) s = fmaf(s, -d * (1.0f / (float)(k + 1)), row[k]);
+    F[M] = s;
+    if (M > 0) {
+      const float e = expf(-T);
+      const float t2 = T + T;
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) F[m] = fmaf(t2, F[m + 1], e) * (1.0f / (float)(2 * m + 1));
+    }
+  } else {
+    const float it = 1.0f / T;
+    F[0] = 0.886226925f * sqrtf(it);
+    if (M > 0) {
+      const float e = expf(-T);
+      const float h = 0.5f * it;
+#pragma unroll
+      for (int m = 0; m < M; ++m) F[m + 1] = ((float)(2 * m + 1) * F[m] - e) * h;
     }
   }
 }

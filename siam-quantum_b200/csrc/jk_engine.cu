@@ -268,6 +268,7 @@ struct sqb200_jk {
   void* d_pairbase = nullptr;   // one allocation holding the pair classes' device arrays
   size_t pairbase_bytes = 0;
   double* d_boys = nullptr;
+  float* d_boysf = nullptr;   // the Boys table in FP32 (mixed-precision forms)
   int* d_shfirst = nullptr;   // per shell first function
   int* d_shn = nullptr;       // per shell function count
   double *d_PA = nullptr, *d_PB = nullptr, *d_PT = nullptr, *d_PM = nullptr;
@@ -1103,6 +1104,7 @@ SegLaunch seg_single(sqb200_jk* c, const sqb200_jk::Work* w, size_t s, const dou
   a.PA = dPA; a.PB = dPB; a.PT = c->d_PT; a.PM = c->d_PM;
   a.Jacc = c->d_J; a.KAacc = c->d_KA; a.KBacc = c->d_KB;
   a.boys_tab = c->d_boys;
+  a.boys_tab_f = c->d_boysf;
   a.counters = c->d_counters + 4 * v;
   a.bra_prims_f = B.d_primsf; a.ket_prims_f = T.d_primsf;
   a.mols = c->d_mol;
@@ -1353,6 +1355,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   for (int s = 0; s < c->ns; ++s) { fst[s] = c->shells[s].first; nf[s] = c->shells[s].nfunc; }
   Carve cv;
   cv.add(&c->d_boys, tab.size() * sizeof(double));
+  cv.add(&c->d_boysf, tab.size() * sizeof(float));
   cv.add(&c->d_shfirst, c->ns * sizeof(int));
   cv.add(&c->d_shn, c->ns * sizeof(int));
   for (double** m : {&c->d_PA, &c->d_PB, &c->d_PT, &c->d_J, &c->d_KA, &c->d_KB, &c->d_JT, &c->d_KAo, &c->d_KBo})
@@ -1368,6 +1371,8 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   }
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = h2d(c->d_boys, tab.data(), tab.size() * sizeof(double), c->stream);
+  std::vector<float> tabf(tab.begin(), tab.end());
+  if (e == cudaSuccess) e = h2d(c->d_boysf, tabf.data(), tabf.size() * sizeof(float), c->stream);
   if (e == cudaSuccess) e = h2d(c->d_shfirst, fst.data(), c->ns * sizeof(int), c->stream);
   if (e == cudaSuccess) e = h2d(c->d_shn, nf.data(), c->ns * sizeof(int), c->stream);
   if (e != cudaSuccess) { sqb200_jk_destroy(c); return fail(SQB200_ECUDA, cudaGetErrorString(e)); }
@@ -2185,6 +2190,7 @@ SegLaunch seg_batch(sqb200_batch* b, size_t s, const double* dPA, const double* 
   a.PA = dPA; a.PB = dPB; a.PT = b->d_PT; a.PM = b->d_PM;
   a.Jacc = b->d_J; a.KAacc = b->d_KA; a.KBacc = b->d_KB;
   a.boys_tab = b->mols[0]->d_boys;
+  a.boys_tab_f = b->mols[0]->d_boysf;
   a.counters = b->d_counters + 4 * (uhf * 2 * K_ + v);
   a.mols = b->d_mols;
   a.same_class = K.bra_cls == K.ket_cls;

@@ -14,7 +14,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsqb200.so")
+# the library this package loads: the one built beside it, unless SQB200_LIB names another build
+LIB_PATH = os.environ.get("SQB200_LIB") or os.path.join(HERE, "libsqb200.so")
 
 _lib = None
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")

@@ -7,7 +7,9 @@ substitutes the monopole values (computeQuartetMPole, src/matrix.c:3945-3949) fo
 quartets whose 1.5^exponent * maxPShell falls below the fixed cutoff.  The visits here follow
 the shape of its 3STEP schedule: a full density at a loose cutoff, then difference densities at
 tightening cutoffs.  Every visit must match the reference's element by element at 1e-10 (the
-plain-FP64 bar), which holds only if the substitution decisions are the same."""
+plain-FP64 bar) and at 1e-7 of each visit's own magnitude, which holds only if the substitution
+decisions are the same; the same visits without substitution differ by 1e-7 to 1e-4 of their
+magnitude, so the mode is exercised."""
 import os
 import tempfile
 
@@ -21,13 +23,15 @@ port = load_oracle()
 
 
 def _visits(n, P0, seed):
+    """A full density, then difference densities shrinking as an SCF's do, at the tightening
+    fixed cutoffs of a 3STEP schedule."""
     rng = np.random.default_rng(seed)
 
     def sym(scale):
         A = rng.normal(size=(n, n)) * scale
         return A + A.T
 
-    return [P0, sym(0.02), sym(0.005), sym(1e-3)], [1e-7, 1e-7, 1e-9, 1e-10]
+    return [P0, sym(1e-2), sym(1e-4), sym(1e-6), sym(1e-8)], [1e-7, 1e-7, 1e-9, 1e-10, 1e-10]
 
 
 @pytest.mark.gpu
@@ -53,14 +57,20 @@ def test_multipole_visits_match_reference(case, max_mem):
         JT, KA, _ = eng.build(P, restricted=True, scf_cutoff=1e-10, fixed_cutoff=c,
                               dscreen_rmax=memcut if v == 0 else float("inf"))
         J0, K0 = ref[v]
-        assert np.abs(JT - J0).max() <= TOL, (case, max_mem, v, np.abs(JT - J0).max())
-        assert np.abs(KA - K0).max() <= TOL, (case, max_mem, v, np.abs(KA - K0).max())
+        # 1e-10 absolute, and 1e-7 of the visit's own scale: the later visits' difference
+        # densities are small, and a substitution decision taken differently moves their J/K
+        # by 1e-4 of their size
+        scale = max(np.abs(J0).max(), np.abs(K0).max())
+        for M, M0 in ((JT, J0), (KA, K0)):
+            err = np.abs(M - M0).max()
+            assert err <= TOL and err <= 1e-7 * scale, (case, max_mem, v, err, scale)
         if v > 0:
-            # the same visit without substitution differs: the mode is really exercised
+            # the same visit with every quartet exact: the difference, far above the rounding
+            # of these matrices, shows that quartets were substituted
             ex = sqb.JKEngine(b, schwarz=g["schwarz"])
             JX, KX, _ = ex.build(P, restricted=True, scf_cutoff=1e-10, fixed_cutoff=c, dscreen_rmax=float("inf"))
             ex.close()
-            substituted = max(substituted, np.abs(JX - J0).max())
+            substituted = max(substituted, max(np.abs(JX - J0).max(), np.abs(KX - K0).max()) / scale)
     if max_mem == 0:
-        assert substituted > TOL, substituted
+        assert substituted > 1e-12, substituted
     eng.close()
