@@ -106,7 +106,8 @@ constexpr int ERR_UNKNOWN = 121;
 // Monopole-monopole value of the function-pair quartet (pq|rs) (computeQuartetMPole): charges
 // times the inverse distance between the pairs' charge centres, 0 when the squared distance
 // is below MULTIPOLE_R2_CUTOFF; the same operations in the same order, without contractions.
-__device__ __forceinline__ double mpole_value(const double* __restrict__ mp, int N, int p, int q, int r, int s) {
+// Not inlined: the multipole mode is rare and its callers are unrolled over whole blocks.
+static __device__ __noinline__ double mpole_value(const double* __restrict__ mp, int N, int p, int q, int r, int s) {
   const double* m1 = mp + 4 * ((long long)p * N + q);
   const double* m2 = mp + 4 * ((long long)r * N + s);
   const double dx = __dadd_rn(m1[1], -m2[1]), dy = __dadd_rn(m1[2], -m2[2]), dz = __dadd_rn(m1[3], -m2[3]);
