@@ -74,6 +74,10 @@ PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the
 # the wide form stages the ket primitive fields a pass reads in shared memory, one record ahead
 # (cp.async double buffer, thread-private slots), instead of reading them from global memory
 STAGE_WIDE = int(os.environ.get("SQB_STAGE_WIDE", "0"))
+# the Boys-function table columns a kernel reads, staged in shared memory once per CTA: the
+# Taylor rows are gathered at each lane's own T, which from global memory touches one L1 line
+# per lane and load
+BOYS_SMEM = int(os.environ.get("SQB_BOYS_SMEM", "0"))
 F32_MAX_L = 6               # mixed-precision kernels for classes up to this total angular momentum
 MIN_BLOCKS = int(os.environ.get("SQB_MINB", "0"))   # __launch_bounds__ min CTAs per SM (0 = none)
 # the same bound for the FP64 narrow-tile form only (its state is smallest, so a register cap
@@ -236,6 +240,20 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
 
     em = Emitter()
     out = []
+    # Boys orders of the passes (the highest Hermite order each pass needs)
+    lps = []
+    for blk in blocks:
+        need_ = {(h[0] + t, h[1] + u, h[2] + v) for cd in blk for (t, u, v) in nz(fk[cd]) for h in Hb}
+        lps.append(max(sum(x) for x in need_))
+    BS = bool(BOYS_SMEM)
+    bnt = 6 if F32 else 9                                   # Taylor terms of boysf / boys
+    bc0, bnc = min(lps), max(lps) - min(lps) + bnt         # staged table columns
+    prologue = []
+    if BS:
+        prologue = ["__shared__ %s sboys[BOYS_NGRID * %d];   // Boys table columns %d..%d" % (RT, bnc, bc0, bc0 + bnc - 1),
+                    "for (int x = threadIdx.x; x < BOYS_NGRID * %d; x += blockDim.x)" % bnc,
+                    "  sboys[x] = a.boys_tab%s[(x / %d) * BOYS_NCOL + %d + x %% %d];" % ("_f" if F32 else "", bnc, bc0, bnc),
+                    "__syncthreads();"]
     minb = MIN_BLOCKS_NARROW if (MIN_BLOCKS_NARROW and suffix == "" and not F32) else MIN_BLOCKS
     out.append('extern "C" __global__ void __launch_bounds__(%s)' % (
         "%d, %d" % (CTA, minb) if minb else "%d" % CTA))
@@ -408,13 +426,19 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
         Lp = max(sum(x) for x in need)          # highest Hermite order this pass needs
         if F32:
             em("float F[%d];" % (Lp + 1))
-            em("sqb::boysf<%d>(T, a.boys_tab_f, F);" % Lp)
+            if BS:
+                em("sqb::boys_s<%d, %d>(T, sboys + %d, F);" % (Lp, bnc, Lp - bc0))
+            else:
+                em("sqb::boysf<%d>(T, a.boys_tab_f, F);" % Lp)
             em("const float s0 = TWO_PI_2_5F * rs;")
             em("const float m2a = -2.0f * alpha;")
             em("float w = s0;")
         else:
             em("double F[%d];" % (Lp + 1))
-            em("sqb::boys<%d>(T, a.boys_tab, F);" % Lp)
+            if BS:
+                em("sqb::boys_s<%d, %d>(T, sboys + %d, F);" % (Lp, bnc, Lp - bc0))
+            else:
+                em("sqb::boys<%d>(T, a.boys_tab, F);" % Lp)
             em("const double s0 = TWO_PI_2_5 * rs;")
             em("const double m2a = -2.0 * alpha;")
             em("double w = s0;")
@@ -498,14 +522,14 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     em("sqb::count_add(a.counters + 1, nprimq);")
     em("sqb::count_add(a.counters + 2, nflush);")
     em("sqb::count_add(a.counters + 3, (ok && pass == 0) ? 1ull : 0ull);")
-    out.extend(persistent_body(em.lines))
+    out.extend(persistent_body(em.lines, prologue))
     out.append("}")
     meta = {"name": name, "bra": bra, "ket": ket, "spin": spin, "nab": nab, "ncd": ncd,
             "neb": len(layb), "nek": len(layk), "Lt": Lt, "flops": fl}
     return "\n".join(out) + "\n", meta
 
 
-def persistent_body(lines):
+def persistent_body(lines, prologue=()):
     """Wrap a class kernel's body in the work loop of the persistent launch.  A work unit is one
     (work item, pass) pair.  With a.queue null the CTA runs the unit (blockIdx.x, blockIdx.y)
     and stops (one CTA per unit); otherwise a grid of about one CTA per resident slot takes
@@ -515,7 +539,7 @@ def persistent_body(lines):
     time work on different items: the passes of one item digest into the same exchange
     elements, and running them side by side would queue their atomics on the same addresses."""
     body = [l.replace("blockIdx.x", "qi_").replace("blockIdx.y", "qp_") for l in lines]
-    out = ["  __shared__ int q_next;",
+    out = ["  __shared__ int q_next;"] + ["  " + l for l in prologue] + [
            "  const bool persistent = a.queue != nullptr;",
            "  for (int round = 0;; ++round) {",
            "    int qi_, qp_;",

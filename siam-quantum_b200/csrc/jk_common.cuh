@@ -177,6 +177,38 @@ __device__ __forceinline__ void boysf(float T, const float* __restrict__ tab, fl
   }
 }
 
+// F_0..F_M at T, as boys<M> (R = double) or boysf<M> (R = float), reading the Taylor rows from
+// a copy of the table's columns in shared memory: s points at column M of a table of NC columns
+// per grid row (the staged columns start at some order c0 <= M; s = staged + M - c0).
+template <int M, int NC, class R>
+__device__ __forceinline__ void boys_s(R T, const R* __restrict__ s, R* F) {
+  constexpr int NT = sizeof(R) == 8 ? BOYS_NTAY : 6;
+  if (T < (R)BOYS_TMAX) {
+    const int g = (int)rint(T * (R)BOYS_INV_H);
+    const R d = T - g * (R)BOYS_H;
+    const R* row = s + g * NC;
+    R acc = row[NT - 1];
+#pragma unroll
+    for (int k = NT - 2; k >= 0; --k) acc = fma(acc, -d * ((R)1 / (R)(k + 1)), row[k]);
+    F[M] = acc;
+    if (M > 0) {
+      const R e = exp(-T);
+      const R t2 = T + T;
+#pragma unroll
+      for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * ((R)1 / (R)(2 * m + 1));
+    }
+  } else {
+    const R it = (R)1 / T;
+    F[0] = (R)0.88622692545275801365 * sqrt(it);
+    if (M > 0) {
+      const R e = exp(-T);
+      const R h = (R)0.5 * it;
+#pragma unroll
+      for (int m = 0; m < M; ++m) F[m + 1] = ((R)(2 * m + 1) * F[m] - e) * h;
+    }
+  }
+}
+
 // Warp-aggregated 64-bit counter increment.
 __device__ __forceinline__ void count_add(unsigned long long* c, unsigned long long v) {
 #pragma unroll
