@@ -581,7 +581,7 @@ def run_reference_split(args, atoms, bname, PA, desc, procs, sqb):
 # kernel, from one `ncu --set full` capture of the same workload; the summary with its command
 # is profiles/<kernel>_<workload>.md.  Kernels without a capture report null.
 TRAFFIC = {("benzene", "jk_DL_LL_R"): 912384, ("benzene", "jk_DL_LL_R_w"): 845312,
-           ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768}
+           ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768, ("c60", "jk_LL_LL_R_w"): 20852224}
 
 
 def max_over_ranks(dist, t_local, device):
@@ -716,7 +716,8 @@ def run_ours(args, sqb):
     if tb is not None and not dom32:
         roof["traffic"] = tb
         roof["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/%s" % (
-            {"benzene": "jk_DL_LL_R_forms_benzene_631gs.md", "c60-synthetic": "jk_LL_LL_R_w_c60_631g.md"}.get(
+            {"benzene": "jk_DL_LL_R_forms_benzene_631gs.md", "c60-synthetic": "jk_LL_LL_R_w_c60_631g_synthetic.md",
+             "c60": "jk_LL_LL_R_w_c60_631g_refdensity.md"}.get(
                 args.workload, args.workload))
     line = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
