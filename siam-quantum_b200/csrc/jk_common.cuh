@@ -17,7 +17,10 @@
 #define BOYS_NGRID  361      // grid points T0 = 0, 0.1, ..., 36.0
 #define BOYS_MMAX   8        // highest order requested by a kernel ((dd|dd))
 #define BOYS_NTAY   9        // Taylor terms
-#define BOYS_NCOL   (BOYS_MMAX + BOYS_NTAY)   // columns m = 0..16 per grid row
+// columns m = 0..17 per grid row: a row is 144 bytes (a multiple of 16), so the Taylor values of
+// any order M (columns M..M+8, read from the even column at or below M) come in five 16-byte
+// loads; each lane gathers its own row, one L1 sector per load
+#define BOYS_NCOL   (BOYS_MMAX + BOYS_NTAY + 1)
 
 #define TWO_PI_2_5  34.986836655249725     // 2 pi^(5/2)
 #define PRIM_CUTOFF 1.0e-15                // reference src/int.h:19
@@ -122,7 +125,15 @@ __device__ __forceinline__ void boys(double T, const double* __restrict__ tab, d
   if (T < BOYS_TMAX) {
     const int g = __double2int_rn(T * BOYS_INV_H);
     const double d = T - g * BOYS_H;          // |d| <= BOYS_H/2
-    const double* row = tab + g * BOYS_NCOL + M;
+    const double2* r2 = reinterpret_cast<const double2*>(tab + g * BOYS_NCOL + (M & ~1));
+    double v[BOYS_NTAY + 1];
+#pragma unroll
+    for (int q = 0; q < (BOYS_NTAY + 1) / 2; ++q) {
+      const double2 t = __ldg(r2 + q);
+      v[2 * q] = t.x;
+      v[2 * q + 1] = t.y;
+    }
+    const double* row = v + (M & 1);          // row[k] = F_{M+k}(T0)
     // Horner in -d with 1/k! folded in: sum_k row[k] (-d)^k / k!
     double s = row[BOYS_NTAY - 1];
 #pragma unroll
@@ -154,7 +165,15 @@ __device__ __forceinline__ void boysf(float T, const float* __restrict__ tab, fl
   if (T < (float)BOYS_TMAX) {
     const int g = __float2int_rn(T * (float)BOYS_INV_H);
     const float d = T - g * (float)BOYS_H;
-    const float* row = tab + g * BOYS_NCOL + M;
+    const float2* r2 = reinterpret_cast<const float2*>(tab + g * BOYS_NCOL + (M & ~1));
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float2 t = __ldg(r2 + q);
+      v[2 * q] = t.x;
+      v[2 * q + 1] = t.y;
+    }
+    const float* row = v + (M & 1);           // row[k] = F_{M+k}(T0), k < 6
     float s = row[5];
 #pragma unroll
     for (int k = 4; k >= 0; --k) s = fmaf(s, -d * (1.0f / (float)(k + 1)), row[k]);
