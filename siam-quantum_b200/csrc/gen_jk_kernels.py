@@ -50,9 +50,11 @@ PAIRS = [a + b for a in "SLPD" for b in "SLPD" if TYPE_ID[a] >= TYPE_ID[b]]
 # bra/ket orientation: the larger pair (by functions, then L) is the bra
 PAIR_ORDER = sorted(PAIRS, key=lambda p: (len(COMP[p[0]]) * len(COMP[p[1]]), LMAX[p[0]] + LMAX[p[1]], p))
 STATE_MAX = int(os.environ.get("SQB_STATE_MAX", "64"))   # doubles of G + out accumulators per pass
-# the mixed (FP32) form: floats of G + out per pass (a float takes one register; measured on
-# LL|LL: 64 floats -> 8 passes at 188 registers, 96 -> 6 passes at 242, 128 -> spills)
-STATE_MAX_F32 = int(os.environ.get("SQB_STATE_MAX_F32", "96"))
+# the mixed (FP32) form: floats of G + out per pass (a float takes one register).  LL|LL: 64
+# floats -> 8 passes at 188 registers, 96 -> 6 passes at 242, 128 -> 4 passes at 255 with 132 B
+# of spills; on C60 (tau 1e-5) 128 floats took the build from 64.4 to 53.5 ms: as for the FP64
+# forms, fewer passes pay more than the spills cost
+STATE_MAX_F32 = int(os.environ.get("SQB_STATE_MAX_F32", "128"))
 # the wide tile: a second FP64 form of every class whose passes it merges (fewer passes, each
 # re-deriving the Boys function and R for more ket functions, at more registers); which form a
 # class runs is chosen by measurement (sqb200_jk_autotune)
