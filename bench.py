@@ -259,7 +259,7 @@ def ref_scf_sample(mols, basis_name, procs, sqb, timeout=600):
     return wall, energies
 
 
-def ref_scf_iterations(mol, basis_name, sqb, timeout=600):
+def ref_scf_iterations(mol, basis_name, sqb, timeout=3600):
     """The reference's own SCF (oracle/_ref/sqref scf, 1STEP, SCFConv 1e-8) of one molecule:
     (iterations it ran, converged) -- uhf() stops at its iteration cap without converging."""
     sqref = os.path.join(ROOT, "oracle", "_ref", "sqref")
@@ -380,19 +380,23 @@ def run_organics(args, sqb):
                              "packed %.0f MB density/J/K arrays and the pair data is re-read per class "
                              "launch)" % (8 * tot / 1e6)},
             "iterations": iters, "converged": conv, "unconverged": [len(mols) - c for c in conv],
+            "unconverged_molecules": [{"molecule": int(i), "nbf": nbfs[i]} for i in np.nonzero(~cv)[0]],
             "max_abs_dE_between_solves_converged": dE_rerun,
             "last_solve_device_split": split,
             "iterations_per_molecule": {"mean": float(np.mean(bs_iters)), "max": int(np.max(bs_iters))},
             "batched_jk": jk, "one_at_a_time_gpu": one, "e2e": e2e, "gpu_launches": None}
     if world == 1 and not args.no_cpu_baseline:
-        # the molecules that did not converge here (<= 120 functions, at most 4): does the
-        # reference's own SCF converge them within its 80 iterations?
-        unc = [i for i in np.nonzero(~cv)[0] if nbfs[i] <= 120][:4]
+        # the smallest molecules that did not converge here (at most 3): does the reference's own
+        # SCF converge them within its 80 iterations?
+        unc = sorted(np.nonzero(~cv)[0], key=lambda i: nbfs[i])[:3]
         try:
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(max_workers=max(1, len(unc))) as ex:
+                outs = list(ex.map(lambda i: ref_scf_iterations(mols[i], bname, sqb), unc))
             line["reference_on_unconverged"] = [
                 {"molecule": int(i), "nbf": nbfs[i], "iterations_here": int(bs_iters[i]),
                  "reference_iterations": it, "reference_converged": ok}
-                for i, (it, ok) in ((i, ref_scf_iterations(mols[i], bname, sqb)) for i in unc)]
+                for i, (it, ok) in zip(unc, outs)]
         except Exception as e:
             line["reference_on_unconverged"] = "failed: %s" % e
         try:
