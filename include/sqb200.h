@@ -23,7 +23,8 @@ extern "C" {
 
 #define SQB200_OK            0
 #define SQB200_EINVAL       -1   /* bad argument                                  */
-#define SQB200_EUNSUPPORTED -2   /* shell type beyond d, or non-canonical order   */
+#define SQB200_EUNSUPPORTED -2   /* function above f (l+m+n > 3), or a mode the basis */
+                                 /* does not support (see the entry point)           */
 #define SQB200_ENOMEM       -3   /* device or host allocation failed              */
 #define SQB200_ECUDA        -4   /* CUDA runtime error                            */
 #define SQB200_ENODEV       -5   /* no usable CUDA device                         */
@@ -34,7 +35,11 @@ typedef struct sqb200_jk sqb200_jk;   /* opaque per-basis device context */
  * Replaces the first-visit set-up of GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3830-3886:
  * genGTOShell, sortGTOShell, shell-level Schwarz).  `schwarz` is the basis-level Schwarz
  * matrix of create_Schwarz (src/matrix.c:389) the caller already holds (the argument
- * `Schwarz` of uhf_getGMatrix, src/uhf.c:112); pass NULL to compute it on the device. */
+ * `Schwarz` of uhf_getGMatrix, src/uhf.c:112); pass NULL to compute it on the device.
+ * Functions up to f (l+m+n <= 3) in shells of up to 16 functions: s, sp, p and d shells in the
+ * reference's component order run in the generated class kernels, every other shell (f, as
+ * read_GAMESS_BasisSet lays it out, src/basis.c:488-499, or another layout) on the generic
+ * path; a function above f returns SQB200_EUNSUPPORTED. */
 int sqb200_jk_create(sqb200_jk **ctx, int nbf, const int *nprim, const int *lmn,
                      const double *xyz, const double *exps, const double *ncoefs,
                      const double *schwarz, int device);
@@ -71,7 +76,7 @@ int sqb200_jk_build_device(sqb200_jk *ctx, const double *dPA, const double *dPB,
  * device array of about 4 MB that every GPU loading the library keeps until exit; its device
  * address is looked up by sqb200_jk_create, with the context's device current.
  * Limits: nbf <= 256 and at most 65536 work items; larger inputs return SQB200_EINVAL with
- * a message.  The context itself (sqb200_jk_create) must already exist.  Every call shares
+ * a message.  A basis with f shells returns SQB200_EUNSUPPORTED.  The context itself (sqb200_jk_create) must already exist.  Every call shares
  * the one array, so calls that overlap on the GPU (other streams, other threads, other
  * contexts on the same device) race; serialise them.  Buffers are device pointers on the
  * context's device, enqueued on `stream` (NULL = the context's stream); not synchronised.
@@ -171,7 +176,8 @@ typedef struct sqb200_batch sqb200_batch;
 /* Join nmol contexts (sqb200_jk_create, all on one device) into a batch.  The batch copies
  * their pair data into merged per-class arrays; the contexts must outlive the batch (their
  * Boys table, shells and FP32 threshold are read).  Packed layout of every batched matrix:
- * molecule m's nbf_m x nbf_m row-major block starts at element off[m] (sqb200_batch_offsets). */
+ * molecule m's nbf_m x nbf_m row-major block starts at element off[m] (sqb200_batch_offsets).
+ * A context whose basis has f shells returns SQB200_EUNSUPPORTED. */
 int sqb200_batch_create(sqb200_batch **batch, int nmol, sqb200_jk *const *ctxs);
 int sqb200_batch_destroy(sqb200_batch *batch);
 

@@ -30,7 +30,7 @@ COMPONENTS = {
 
 BASIS_NAMES = {"sto3g": "sto3g", "sto-3g": "sto3g", "321g": "321g", "3-21g": "321g",
                "631g": "631g", "6-31g": "631g", "631g*": "631g_star", "631g_star": "631g_star",
-               "6-31g*": "631g_star"}
+               "6-31g*": "631g_star", "dzp": "dzp", "qzp": "qzp_gh", "qzp-gh": "qzp_gh", "qzp_gh": "qzp_gh"}
 
 
 def _dfact(n):

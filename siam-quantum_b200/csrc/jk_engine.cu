@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "jk_common.cuh"
+#include "jk_generic.cuh"
 #include "jk_registry.h"
 #include "../../include/sqb200.h"
 
@@ -113,12 +114,15 @@ struct Staged : Carve {
 
 // ---------------------------------------------------------------- Boys table (host)
 
-// F_m(T0) for the grid T0 = g*BOYS_H, m = 0..BOYS_NCOL-1, in long double:
+}  // namespace
+
+namespace sqb {
+// F_m(T0) for the grid T0 = g*BOYS_H, m = 0..ncol-1, in long double:
 // the top order by its convergent series e^-T sum_i (2T)^i / ((2m+1)(2m+3)...(2m+2i+1)),
 // the rest by downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1).
-std::vector<double> make_boys_table() {
-  std::vector<double> tab(BOYS_NGRID * BOYS_NCOL);
-  const int top = BOYS_NCOL - 1;
+std::vector<double> boys_table(int ncol) {
+  std::vector<double> tab(BOYS_NGRID * ncol);
+  const int top = ncol - 1;
   for (int g = 0; g < BOYS_NGRID; ++g) {
     const long double T = (long double)g * (long double)BOYS_H;
     long double term = 1.0L / (2 * top + 1), sum = 0.0L;
@@ -129,18 +133,25 @@ std::vector<double> make_boys_table() {
     }
     const long double e = expl(-T);
     long double F = e * sum;
-    std::vector<long double> col(BOYS_NCOL);
+    std::vector<long double> col(ncol);
     col[top] = F;
     for (int m = top - 1; m >= 0; --m) col[m] = (2.0L * T * col[m + 1] + e) / (2 * m + 1);
-    for (int m = 0; m < BOYS_NCOL; ++m) tab[g * BOYS_NCOL + m] = (double)col[m];
+    for (int m = 0; m < ncol; ++m) tab[g * ncol + m] = (double)col[m];
   }
   return tab;
 }
+}  // namespace sqb
+
+namespace {
+
+std::vector<double> make_boys_table() { return sqb::boys_table(BOYS_NCOL); }
 
 // ---------------------------------------------------------------- shells
 
 struct Shell {
   int first, nfunc, type, nprim;
+  int gen;                 // 1: its pairs take the generic path (jk_generic.cu)
+  int lmax;                // highest l+m+n of its functions
   double x, y, z;
   double exps[32];
   double coef[32][16];
@@ -183,17 +194,30 @@ int build_shells(int nbf, const int* nprim, const int* lmn, const double* xyz,
       ++s.nfunc;
       ++q;
     }
+    // the reference's type by function count (genGTOShell, src/matrix.c:2527-2535: S, P, L, D,
+    // F = 4 for ten functions, X = 6 otherwise); it fixes the shell order (sortGTOShell)
     switch (s.nfunc) {
       case 1: s.type = 0; break;
       case 4: s.type = 1; break;
       case 3: s.type = 2; break;
       case 6: s.type = 3; break;
-      default: return fail(SQB200_EUNSUPPORTED, "shell with " + std::to_string(s.nfunc) + " functions (only s, sp, p, d supported)");
+      case 10: s.type = 4; break;
+      default: s.type = 6; break;
     }
-    for (int f = 0; f < s.nfunc; ++f)
-      for (int d = 0; d < 3; ++d)
-        if (s.lmn[f][d] != kComp[s.type][f][d])
-          return fail(SQB200_EUNSUPPORTED, "shell components not in the canonical Cartesian order");
+    // s, sp, p and d shells in the canonical component order run in the generated class kernels;
+    // every other shell (f, or another layout) on the generic path
+    s.gen = s.type > 3 ? 1 : 0;
+    for (int f = 0; f < s.nfunc; ++f) {
+      int l = 0;
+      for (int d = 0; d < 3; ++d) {
+        if (s.lmn[f][d] < 0) return fail(SQB200_EINVAL, "negative angular index");
+        l += s.lmn[f][d];
+        if (!s.gen && s.lmn[f][d] != kComp[s.type][f][d]) s.gen = 1;
+      }
+      if (l > sqb::kGenLmax)
+        return fail(SQB200_EUNSUPPORTED, "function with l+m+n = " + std::to_string(l) + " (f, 3, is the highest supported)");
+      s.lmax = std::max(s.lmax, l);
+    }
     sh.push_back(s);
     p = q;
   }
@@ -201,15 +225,15 @@ int build_shells(int nbf, const int* nprim, const int* lmn, const double* xyz,
   return SQB200_OK;
 }
 
-// 1-D Hermite expansion coefficients E^{ij}_t (i <= 2, j <= 2, t <= i+j) of a Gaussian pair
-// product relative to the product centre: E^{00}_0 = 1,
+// 1-D Hermite expansion coefficients E^{ij}_t (i <= 3, j <= 3, t <= i+j: up to f) of a
+// Gaussian pair product relative to the product centre: E^{00}_0 = 1,
 // E^{i+1,j}_t = E^{ij}_{t-1}/(2p) + XPA E^{ij}_t + (t+1) E^{ij}_{t+1}, likewise for j.
-void hermite_e(double p, double xpa, double xpb, double E[3][3][5]) {
-  memset(E, 0, sizeof(double) * 45);
+void hermite_e(double p, double xpa, double xpb, double E[4][4][7]) {
+  memset(E, 0, sizeof(double) * 4 * 4 * 7);
   const double h = 0.5 / p;
   E[0][0][0] = 1.0;
-  for (int i = 0; i <= 2; ++i)
-    for (int j = 0; j <= 2; ++j) {
+  for (int i = 0; i <= 3; ++i)
+    for (int j = 0; j <= 3; ++j) {
       if (i == 0 && j == 0) continue;
       const bool up_i = i > 0;
       const int si = up_i ? i - 1 : i, sj = up_i ? j : j - 1;
@@ -288,6 +312,8 @@ struct sqb200_jk {
     sqb::WorkItem* d_items = nullptr;
     int* d_er = nullptr;          // multipole mode: per item, the error-bank slot of its first ket
     int total = 0;
+    sqb::GenItem* d_gitems = nullptr;   // the generic path's items (shells outside the classes)
+    int gtotal = 0;
   };
   // key: outer cutoff, fixed cutoff, FP32 threshold, multipole mode
   std::map<std::tuple<double, double, double, int>, Work> work;
@@ -328,6 +354,8 @@ struct sqb200_jk {
   signed char* d_erbank = nullptr;
   long long er_total = -1;
   double er_outer = -1.0;
+  // quartets with a shell outside the generated classes (f shells and other layouts)
+  sqb::GenPath gen;
 };
 
 namespace {
@@ -506,7 +534,8 @@ __global__ void k_schwarz(const sqb::PairRec* __restrict__ pairs, const double* 
 //   T = -1/2 sum_axes [ j(j-1) S(i,j-2) - 2b(2j+1) S(i,j) + 4b^2 S(i,j+2) ] x (other axes' S)
 //   V = -sum_C Z_C 2pi/p c K sum_tuv E_t E_u E_v R_tuv(p, P - C)
 
-__device__ void oe_hermite(double p, double xpa, double xpb, int la, int lb, double E[3][5][7]) {
+// E[i][j][t] for i <= la <= 3, j <= lb <= 5 (f functions, plus 2 for the kinetic term), t <= i+j
+__device__ void oe_hermite(double p, double xpa, double xpb, int la, int lb, double E[4][6][9]) {
   const double h = 0.5 / p;
   for (int i = 0; i <= la; ++i)
     for (int j = 0; j <= lb; ++j)
@@ -541,7 +570,7 @@ __global__ void k_oneint(int nbf, const int* __restrict__ nprim, const int* __re
   const double* A = xyz + 3 * pa;
   const double* B = xyz + 3 * pb;
   double s = 0.0, t = 0.0, v = 0.0;
-  double Ex[3][5][7], Ey[3][5][7], Ez[3][5][7];
+  double Ex[4][6][9], Ey[4][6][9], Ez[4][6][9];
   double Rc[165], Rn[165], F[9];
   const double ab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
   for (int i = 0; i < nprim[pa]; ++i)
@@ -555,7 +584,7 @@ __global__ void k_oneint(int nbf, const int* __restrict__ nprim, const int* __re
       const double sq = sqrt(M_PI / p);
       // 1-D overlaps S_d(i, j) = E^{ij}_0 sqrt(pi/p)
       double sd[3], td[3];
-      double (*E[3])[5][7] = {Ex, Ey, Ez};
+      double (*E[3])[6][9] = {Ex, Ey, Ez};
       for (int d = 0; d < 3; ++d) {
         const int ii = la[d], jj = lb[d];
         sd[d] = E[d][ii][jj][0] * sq;
@@ -626,6 +655,7 @@ void build_pairs(sqb200_jk* c) {
   std::vector<Tmp> lists[sqb::kNumPairClasses];
   for (int P = 0; P < ns; ++P)
     for (int Q = 0; Q <= P; ++Q) {
+      if (sh[P].gen || sh[Q].gen) continue;   // the generic path's
       const int k = pair_class_of(sh[P].type, sh[Q].type);
       lists[k].push_back({sch(P, Q), P, Q, sh[P].nprim * sh[Q].nprim});
     }
@@ -668,7 +698,7 @@ void build_pairs(sqb200_jk* c) {
           const double a = A.exps[i], b = B.exps[j], p = a + b;
           const double Px = (a * A.x + b * B.x) / p, Py = (a * A.y + b * B.y) / p, Pz = (a * A.z + b * B.z) / p;
           const double kp = std::exp(-a * b * ab2 / p) / p;
-          double Ex[3][3][5], Ey[3][3][5], Ez[3][3][5];
+          double Ex[4][4][7], Ey[4][4][7], Ez[4][4][7];
           hermite_e(p, Px - A.x, Px - B.x, Ex);
           hermite_e(p, Py - A.y, Py - B.y, Ey);
           hermite_e(p, Pz - A.z, Pz - B.z, Ez);
@@ -709,6 +739,19 @@ void build_pairs(sqb200_jk* c) {
   }
 }
 
+// The generic path's pair data (every shell pair, sorted by the current Schwarz bounds) when
+// the basis has a shell outside the generated classes.
+int setup_generic(sqb200_jk* c, const int* nprim, const int* lmn, const double* ncoefs) {
+  bool any = false;
+  for (const Shell& s : c->shells) any = any || s.gen;
+  c->gen.on = any;
+  if (!any) return SQB200_OK;
+  std::vector<sqb::GenShell> gs;
+  for (const Shell& s : c->shells) gs.push_back({s.first, s.nfunc, s.nprim, s.lmax, s.gen, s.x, s.y, s.z, s.exps});
+  sqb::gen_build_pairs(c->gen, gs, c->schwarz.data(), c->nbf);
+  return sqb::gen_upload(c->gen, c->nbf, nprim, lmn, ncoefs, c->stream);
+}
+
 int compute_schwarz_device(sqb200_jk* c, double* S_host) {
   const size_t nn = (size_t)c->nbf * c->nbf;
   double* dS = c->d_JT;         // scratch: the host-build output buffer, rewritten by every build
@@ -732,6 +775,10 @@ int compute_schwarz_device(sqb200_jk* c, double* S_host) {
     k_schwarz<<<(int)((nthr + 127) / 128), 128, 0, c->stream>>>(pc.d_pairs, pc.d_prims, (int)pc.pairs.size(), pc.stride,
                                                                kNComp[pc.tb], fd, c->d_boys, c->nbf, dS);
     CUDA_OK(cudaGetLastError());
+  }
+  if (c->gen.on) {
+    const int rc = sqb::gen_schwarz(c->gen, c->nbf, dS, c->stream);
+    if (rc) return rc;
   }
   CUDA_OK(cudaMemcpyAsync(S_host, dS, nn * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CUDA_OK(cudaStreamSynchronize(c->stream));
@@ -961,6 +1008,17 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
     CUDA_OK(cudaMalloc(&w.d_items, items.size() * sizeof(sqb::WorkItem)));
     CUDA_OK(h2d(w.d_items, items.data(), items.size() * sizeof(sqb::WorkItem), c->stream));
   }
+  if (c->gen.on) {
+    std::vector<sqb::GenItem> gi;
+    double gcost = 0.0;
+    sqb::gen_items(c->gen, outer, fixed, gi, gcost, mpm ? &er_run : nullptr);
+    if (gi.size() > (size_t)INT_MAX) return fail(SQB200_EINVAL, "generic path: more than 2^31 work items");
+    w.gtotal = (int)gi.size();
+    if (!gi.empty()) {
+      CUDA_OK(cudaMalloc(&w.d_gitems, gi.size() * sizeof(sqb::GenItem)));
+      CUDA_OK(h2d(w.d_gitems, gi.data(), gi.size() * sizeof(sqb::GenItem), c->stream));
+    }
+  }
   if (mpm) {
     if (er_run > INT_MAX) return fail(SQB200_EINVAL, "multipole mode: more than 2^31 quartets survive the outer cutoff");
     if (!ers.empty()) {
@@ -987,6 +1045,9 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
   *out = &ins.first->second;
   return SQB200_OK;
 }
+
+// Profile and class-name index of the generic path's kernel (after the FP64 and FP32 forms).
+const int kGenericKernel = 2 * sqb::kNumClassKernels;
 
 // One class-kernel launch of a work segment, ready to enqueue.
 struct SegLaunch {
@@ -1151,7 +1212,7 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   launch_pmax(dPA, dPB, c->d_PT, c->d_shfirst, c->d_shn, c->ns, n, c->d_PM, st);
   CUDA_OK(cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * 8 * sqb::kNumClassKernels, st));
   if (c->persistent) CUDA_OK(cudaMemsetAsync(c->d_queue, 0, sizeof(unsigned long long) * 2 * sqb::kNumClassKernels, st));
-  c->last_launches = 3 + (int)w->kernel.size();
+  c->last_launches = 3 + (int)w->kernel.size() + (w->gtotal > 0 ? 1 : 0);
   // segments largest first, each on the least-loaded lane (lane 0 = st, the others are side
   // streams forked off st); per-class profiling keeps every launch on st so that each event
   // pair times one kernel alone
@@ -1166,6 +1227,31 @@ int launch_build(sqb200_jk* c, const double* dPA, const double* dPB, int restric
   if (nlanes > 1) {
     CUDA_OK(cudaEventRecord(c->ev_fork, st));
     for (int l = 1; l < nlanes; ++l) CUDA_OK(cudaStreamWaitEvent(c->side[l - 1], c->ev_fork, 0));
+  }
+  if (c->gen.on) {
+    // the generic path's quartets (f shells), on lane 0 ahead of the class kernels
+    sqb::GenBuild gb{dPA, dPB, c->d_PT, c->d_PM, c->d_J, c->d_KA, c->d_KB, n, c->ns, uhf, outer, fixed, dscreen,
+                     nullptr, nullptr, nullptr, nullptr, 0.0};
+    if (c->mp_on && c->d_erbank) {
+      gb.erbank = c->d_erbank;
+      gb.erscr = c->d_erscr;
+      gb.mpole = c->d_mpole;
+      gb.pow15 = c->d_pow15;
+      gb.mp_rmax = c->mp_rmax;
+    }
+    sqb200_jk::Ev ev{kGenericKernel, nullptr, nullptr};
+    if (c->profile && w->gtotal > 0) {
+      CUDA_OK(cudaEventCreate(&ev.a));
+      CUDA_OK(cudaEventCreate(&ev.b));
+      CUDA_OK(cudaEventRecord(ev.a, st));
+    }
+    rc = sqb::gen_launch(c->gen, w->d_gitems, w->gtotal, gb, st);
+    if (rc) return rc;
+    if (ev.a) {
+      CUDA_OK(cudaEventRecord(ev.b, st));
+      c->events.push_back(ev);
+    }
+    used[0] = 1;
   }
   for (size_t s : order) {
     const int lane = (int)(std::min_element(load.begin(), load.end()) - load.begin());
@@ -1298,7 +1384,7 @@ void multipole_table(const sqb200_jk* c, std::vector<double>& tab) {
               const double a = A.exps[k], b = B.exps[l], p = a + b, mu = a * b / p;
               const double Px = (a * A.x + b * B.x) / p, Py = (a * A.y + b * B.y) / p, Pz = (a * A.z + b * B.z) / p;
               const double R2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
-              double Ex[3][3][5], Ey[3][3][5], Ez[3][3][5];
+              double Ex[4][4][7], Ey[4][4][7], Ez[4][4][7];
               hermite_e(p, Px - A.x, Px - B.x, Ex);
               hermite_e(p, Py - A.y, Py - B.y, Ey);
               hermite_e(p, Pz - A.z, Pz - B.z, Ez);
@@ -1348,6 +1434,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   else c->schwarz.assign((size_t)nbf * nbf, 1.0);   // placeholder until the device pass below
   build_pairs(c);
   rc = upload_pairs(c);
+  if (!rc) rc = setup_generic(c, nprim, lmn, ncoefs);
   if (rc) { sqb200_jk_destroy(c); return rc; }
   const size_t nn = (size_t)nbf * nbf;
   std::vector<double> tab = make_boys_table();
@@ -1382,6 +1469,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
     if (rc) { sqb200_jk_destroy(c); return rc; }
     build_pairs(c);
     rc = upload_pairs(c);
+    if (!rc) rc = setup_generic(c, nprim, lmn, ncoefs);
     if (rc) { sqb200_jk_destroy(c); return rc; }
   }
   // the scratch array of sqb200_jk_build_noalloc: its device address on this device, looked up
@@ -1403,7 +1491,8 @@ int sqb200_jk_destroy(sqb200_jk* c) {
     cudaEventDestroy(c->ev_join[i]);
   }
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
-  for (auto& kv : c->work) { cudaFree(kv.second.d_items); cudaFree(kv.second.d_er); }
+  for (auto& kv : c->work) { cudaFree(kv.second.d_items); cudaFree(kv.second.d_er); cudaFree(kv.second.d_gitems); }
+  sqb::gen_free(c->gen);
   if (c->d_mpbase) cudaFree(c->d_mpbase);
   if (c->d_erbase) cudaFree(c->d_erbase);
   for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -1505,8 +1594,15 @@ int sqb200_jk_stats(sqb200_jk* c, long long* out, int n) {
     pq += (long long)h[4 * v + 1];
     fl += (long long)kernel_flops(c, v, &h[4 * v]);
   }
+  if (c->gen.on) {
+    unsigned long long g2[2];
+    CUDA_OK(cudaMemcpy(g2, c->gen.d_counters, sizeof(g2), cudaMemcpyDeviceToHost));
+    q += (long long)g2[0];
+    pq += (long long)g2[1];
+  }
   long long v[6] = {q, pq, fl, (long long)c->ns, 0, (long long)c->last_launches};
   for (int k = 0; k < sqb::kNumPairClasses; ++k) v[4] += (long long)c->cls[k].pairs.size();
+  v[4] += (long long)c->gen.gen_idx.size();
   for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
   return SQB200_OK;
 }
@@ -1523,8 +1619,8 @@ int sqb200_jk_profile(sqb200_jk* c, int enable) {
   CUDA_OK(cudaStreamSynchronize(c->stream));
   for (auto& e : c->events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
   c->events.clear();
-  c->prof_ms.assign(2 * sqb::kNumClassKernels, 0.0);
-  c->prof_launches.assign(2 * sqb::kNumClassKernels, 0);
+  c->prof_ms.assign(kGenericKernel + 1, 0.0);
+  c->prof_launches.assign(kGenericKernel + 1, 0);
   c->profile = enable != 0;
   return SQB200_OK;
 }
@@ -1536,9 +1632,9 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
     CUDA_OK(cudaEventSynchronize(e.b));
     float ms = 0.f;
     CUDA_OK(cudaEventElapsedTime(&ms, e.a, e.b));
-    if (c->prof_ms.size() != (size_t)(2 * sqb::kNumClassKernels)) {
-      c->prof_ms.assign(2 * sqb::kNumClassKernels, 0.0);
-      c->prof_launches.assign(2 * sqb::kNumClassKernels, 0);
+    if (c->prof_ms.size() != (size_t)(kGenericKernel + 1)) {
+      c->prof_ms.assign(kGenericKernel + 1, 0.0);
+      c->prof_launches.assign(kGenericKernel + 1, 0);
     }
     c->prof_ms[e.kernel] += ms;
     c->prof_launches[e.kernel] += 1;
@@ -1548,16 +1644,19 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
   c->events.clear();
   std::vector<unsigned long long> h(8 * sqb::kNumClassKernels);
   CUDA_OK(cudaMemcpy(h.data(), c->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  unsigned long long g2[2] = {0, 0};
+  if (c->gen.on) CUDA_OK(cudaMemcpy(g2, c->gen.d_counters, sizeof(g2), cudaMemcpyDeviceToHost));
   int r = 0;
-  for (int v = 0; v < 2 * sqb::kNumClassKernels && r < max_rows; ++v) {
-    if (c->prof_launches.empty() || c->prof_launches[v] == 0) continue;
+  for (int v = 0; v <= kGenericKernel && r < max_rows; ++v) {
+    if ((int)c->prof_launches.size() <= v || c->prof_launches[v] == 0) continue;
     double* row = rows + 6 * r;
     row[0] = v;
     row[1] = (double)c->prof_launches[v];
     row[2] = c->prof_ms[v];
-    row[3] = kernel_flops(c, v, &h[4 * v]);
-    row[4] = (double)h[4 * v + 1];
-    row[5] = (double)h[4 * v];
+    // (the generic path reports no operation count)
+    row[3] = v == kGenericKernel ? 0.0 : kernel_flops(c, v, &h[4 * v]);
+    row[4] = v == kGenericKernel ? (double)g2[1] : (double)h[4 * v + 1];
+    row[5] = v == kGenericKernel ? (double)g2[0] : (double)h[4 * v];
     ++r;
   }
   *nrows = r;
@@ -1565,6 +1664,7 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
 }
 
 const char* sqb200_jk_class_name(int k) {
+  if (k == kGenericKernel) return "generic (f shells)";
   if (k < 0 || k >= 2 * sqb::kNumClassKernels) return "";
   static std::vector<std::string> names;
   static std::mutex mu;
@@ -1797,6 +1897,7 @@ extern "C" int sqb200_jk_build_noalloc(sqb200_jk* c, const double* dPA, const do
     return fail(SQB200_EINVAL, "sqb200_jk_build_noalloc: " + std::to_string(c->nbf) + " basis functions exceed its limit of " +
                                    std::to_string(kNoAllocMaxNbf));
   if (sqb::kNumClassKernels > kNoAllocMaxKernels) return fail(SQB200_EINVAL, "class table larger than the scratch counters");
+  if (c->gen.on) return fail(SQB200_EUNSUPPORTED, "sqb200_jk_build_noalloc: shells outside s, sp, p, d (f shells)");
   CUDA_OK(cudaSetDevice(c->device));
   unsigned char* base = c->noalloc_base;
   if (!base)
@@ -2014,6 +2115,7 @@ extern "C" int sqb200_batch_create(sqb200_batch** out, int nmol, sqb200_jk* cons
   for (int m = 0; m < nmol; ++m) {
     if (!mols[m]) return fail(SQB200_EINVAL, "sqb200_batch_create: null context");
     if (mols[m]->device != mols[0]->device) return fail(SQB200_EINVAL, "sqb200_batch_create: contexts on different devices");
+    if (mols[m]->gen.on) return fail(SQB200_EUNSUPPORTED, "sqb200_batch_create: shells outside s, sp, p, d (f shells)");
   }
   sqb200_batch* b = new sqb200_batch();
   b->device = mols[0]->device;

@@ -1,0 +1,671 @@
+// The generic J/K path (declarations and scope in jk_generic.cuh): shell quartets with an f
+// shell, or with any shell layout the generated class kernels do not cover, by
+// McMurchie-Davidson with run-time angular momenta.
+//
+// Per quartet (PQ|IJ) and primitive quartet (ij|kl), as the class kernels do it but with loops:
+//   (ab|cd) = sum_tuv E^ab_tuv sum_tau,nu,phi (-1)^(tau+nu+phi) E^cd_tau,nu,phi R_{t+tau,u+nu,v+phi}
+// with E the products of 1-D Hermite coefficients (times contraction weights and
+// exp(-ab|AB|^2/p)/p), R^(0) from the Hermite recursion seeded by
+// 2 pi^(5/2) / sqrt(p+q) (-2 alpha)^n F_n(alpha |PQ|^2).  The ket side is summed over the ket
+// primitives first, G[tuv][cd], and transformed by the bra E once per bra primitive.  The
+// screens (Schwarz outer/fixed cutoffs, density screen below dscreen_rmax, the 1e-15 primitive
+// prefactor cut) and the digestion into J, KA, KB with the 8-fold degeneracy factors are those
+// of the class kernels (GTO_JK_Matrix_Quartet_Parallel and storeQuartetEE, reference
+// src/matrix.c:3773-3986, 2934-3396), so the two paths add into the same accumulators.
+//
+// Layout: one warp per quartet, two warps per CTA; each warp owns a shared-memory region with
+// the Boys-scaled seeds, two buffers of the R recursion (tetrahedral order t+u+v <= 12), the
+// 1-D Hermite tables of its bra and ket primitive pairs, and G and the contracted block O for
+// a chunk of ket function pairs (chunks when a (ff|ff)-sized block does not fit).
+#include "jk_generic.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "jk_common.cuh"
+#include "../../include/sqb200.h"
+
+namespace sqb {
+int set_error(int code, const std::string& msg);
+std::vector<double> boys_table(int ncol);
+}  // namespace sqb
+
+namespace {
+
+using sqb::GenItem;
+using sqb::GenPairRec;
+using sqb::kGenPrimStride;
+
+constexpr int kGenBoysCols = 22;                       // orders 0..21: F_12 + 8 Taylor terms
+constexpr int kGenR = 455;                             // tetrahedral entries with t+u+v <= 12
+constexpr int kGenE1 = 4 * 4 * 7;                      // one axis: E^{ij}_t, i, j <= 3, t <= 6
+constexpr int kGenE = 3 * kGenE1;
+constexpr int kGenWarps = 2;                           // warps per CTA
+constexpr int kGenKets = 16;                           // kets per work item
+constexpr int kGenGO = 2048;                           // doubles for G and O of one chunk
+constexpr int kGenWarpDoubles = 16 + 2 * kGenR + 2 * kGenE + kGenGO;
+constexpr size_t kGenSmem = (size_t)kGenWarps * kGenWarpDoubles * sizeof(double);   // 58,336 B
+
+static_assert(sqb::kGenMmax == 12 && (sqb::kGenMmax + 1) * (sqb::kGenMmax + 2) * (sqb::kGenMmax + 3) / 6 == kGenR,
+              "R table size");
+static_assert(sizeof(GenPairRec) == 56, "pair record layout");
+
+// (t, u, v) of tetrahedral index k: order n = t+u+v, then m = u+v, then v ascending
+struct TuvTable {
+  unsigned int v[kGenR];
+  constexpr TuvTable() : v() {
+    int k = 0;
+    for (int n = 0; n <= sqb::kGenMmax; ++n)
+      for (int m = 0; m <= n; ++m)
+        for (int w = 0; w <= m; ++w) v[k++] = (unsigned)(n - m) | ((unsigned)(m - w) << 8) | ((unsigned)w << 16);
+  }
+};
+__device__ const TuvTable g_tuv = TuvTable();
+
+__device__ __forceinline__ int gtet(int t, int u, int v) {
+  const int n = t + u + v, m = u + v;
+  return n * (n + 1) * (n + 2) / 6 + m * (m + 1) / 2 + v;
+}
+
+struct GenArgs {
+  const GenPairRec* __restrict__ pairs;
+  const double* __restrict__ prims;
+  const int* __restrict__ lmn;
+  const int* __restrict__ foff;
+  const double* __restrict__ ncoef;
+  const double* __restrict__ boys;
+  sqb::GenBuild b;
+  unsigned long long* counters;
+};
+
+__device__ __forceinline__ double gcoef(const GenArgs& a, int f, int k) {
+  return __ldg(a.ncoef + __ldg(a.foff + f) + k);
+}
+
+// 1-D Hermite coefficients E^{ij}_t (i <= la, j <= lb) of a primitive pair along one axis into
+// E[(i*4 + j)*7 + t]:  E^{00}_0 = 1,
+// E^{i+1,j}_t = E^{ij}_{t-1}/(2p) + X_PA E^{ij}_t + (t+1) E^{ij}_{t+1}, likewise in j with X_PB.
+__device__ void gen_e1d(double p, double xpa, double xpb, int la, int lb, double* E) {
+  const double h = 0.5 / p;
+  for (int i = 0; i <= la; ++i)
+    for (int j = 0; j <= lb; ++j) {
+      double* e = E + (i * 4 + j) * 7;
+      if (i == 0 && j == 0) {
+        e[0] = 1.0;
+        continue;
+      }
+      const bool up = i > 0;
+      const double* s = up ? E + ((i - 1) * 4 + j) * 7 : E + (i * 4 + j - 1) * 7;
+      const int ls = i + j - 1;                     // highest t of the source
+      const double X = up ? xpa : xpb;
+      for (int t = 0; t <= i + j; ++t) {
+        double v = t <= ls ? X * s[t] : 0.0;
+        if (t > 0) v += h * s[t - 1];
+        if (t + 1 <= ls) v += (t + 1) * s[t + 1];
+        e[t] = v;
+      }
+    }
+}
+
+// F_n(T) for one order n <= 12: below BOYS_TMAX the 9-term Taylor expansion about the nearest
+// grid point, F_n(T0+d) = sum_k F_{n+k}(T0) (-d)^k / k!, from the table's own column n; above,
+// F_0 = sqrt(pi/T)/2 and the upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T).
+__device__ double gen_boys(int n, double T, const double* __restrict__ tab) {
+  if (T < BOYS_TMAX) {
+    const int g = __double2int_rn(T * BOYS_INV_H);
+    const double d = T - g * BOYS_H;
+    const double* row = tab + g * kGenBoysCols + n;
+    double s = __ldg(row + BOYS_NTAY - 1);
+    for (int k = BOYS_NTAY - 2; k >= 0; --k) s = fma(s, -d * (1.0 / (double)(k + 1)), __ldg(row + k));
+    return s;
+  }
+  const double it = 1.0 / T;
+  double F = 0.88622692545275801365 * sqrt(it);   // sqrt(pi)/2 / sqrt(T)
+  if (n > 0) {
+    const double e = exp(-T), h = 0.5 * it;
+    for (int m = 0; m < n; ++m) F = ((2 * m + 1) * F - e) * h;
+  }
+  return F;
+}
+
+// Seeds base[n] = 2 pi^(5/2)/sqrt(p+q) (-2 alpha)^n F_n(T), n <= L, one lane per order.
+__device__ __forceinline__ void gen_seeds(int L, double alpha, double rs, double T, const double* tab, double* base,
+                                          int lane) {
+  if (lane <= L) {
+    const double m2a = -2.0 * alpha;
+    double w = TWO_PI_2_5 * rs;
+    for (int k = 0; k < lane; ++k) w *= m2a;
+    base[lane] = w * gen_boys(lane, T, tab);
+  }
+}
+
+// R^(0)_{tuv}, t+u+v <= L, from the seeds by the Hermite recursion
+//   R^(n)_{t+1,u,v} = t R^(n+1)_{t-1,u,v} + X R^(n+1)_{t,u,v}   (likewise in u, v),
+// level by level from n = L down to 0, the lanes sharing each level; returns the buffer that
+// holds level 0.  The seeds must be visible to the warp (synchronised) before the call.
+__device__ const double* gen_rtab(int L, double X, double Y, double Z, const double* base, double* b0, double* b1,
+                                  int lane) {
+  double* cur = b0;
+  double* nxt = b1;
+  if (lane == 0) cur[0] = base[L];
+  __syncwarp();
+  for (int n = L - 1; n >= 0; --n) {
+    const int top = L - n;
+    const int cnt = (top + 1) * (top + 2) * (top + 3) / 6;
+    for (int idx = lane; idx < cnt; idx += 32) {
+      const unsigned e = g_tuv.v[idx];
+      const int t = e & 255, u = (e >> 8) & 255, v = e >> 16;
+      double r;
+      if (idx == 0) r = base[n];
+      else if (t > 0) r = X * cur[gtet(t - 1, u, v)] + (t > 1 ? (t - 1) * cur[gtet(t - 2, u, v)] : 0.0);
+      else if (u > 0) r = Y * cur[gtet(t, u - 1, v)] + (u > 1 ? (u - 1) * cur[gtet(t, u - 2, v)] : 0.0);
+      else r = Z * cur[gtet(t, u, v - 1)] + (v > 1 ? (v - 1) * cur[gtet(t, u, v - 2)] : 0.0);
+      nxt[idx] = r;
+    }
+    __syncwarp();
+    double* tmp = cur;
+    cur = nxt;
+    nxt = tmp;
+  }
+  return cur;
+}
+
+// sum_{tau,nu,phi} (-1)^(tau+nu+phi) E_x[tau] E_y[nu] E_z[phi] R_{t+tau,u+nu,v+phi}
+__device__ __forceinline__ double ket_sum(const double* ex, const double* ey, const double* ez, int nx, int ny, int nz,
+                                          int t, int u, int v, const double* R) {
+  double s = 0.0;
+  for (int tau = 0; tau <= nx; ++tau)
+    for (int nu = 0; nu <= ny; ++nu) {
+      double sz = 0.0;
+      for (int ph = 0; ph <= nz; ++ph) {
+        const double r = R[gtet(t + tau, u + nu, v + ph)] * ez[ph];
+        sz += ((tau + nu + ph) & 1) ? -r : r;
+      }
+      s = fma(ex[tau] * ey[nu], sz, s);
+    }
+  return s;
+}
+
+// J, KA (and KB) contributions of one contracted chunk O[ab][cc] (bra function pairs ab, ket
+// function pairs cd = c0 + cc), in the class kernels' convention:
+//   J[pq] += 2 deg sum O PT[ij],  J[ij] += 2 deg sum O PT[pq],
+//   K[p][i] += deg O D[q][j],  K[q][i] += deg O D[p][j],  K[p][j] += deg O D[q][i],
+//   K[q][j] += deg O D[p][i]   (D = PA into KA; PB into KB when unrestricted).
+__device__ void gen_digest(const GenArgs& a, const GenPairRec& A, const GenPairRec& B, double deg, const double* O,
+                           int c0, int nc, int lane) {
+  const int N = a.b.nbf;
+  const int nfP = A.nfP, nfQ = A.nfQ, nfJ = B.nfQ;
+  const int fP = A.fP, fQ = A.fQ, fI = B.fP, fJ = B.fQ;
+  const int nA = nfP * nfQ;
+  const double* __restrict__ PT = a.b.PT;
+  const double s2 = 2.0 * deg;
+  for (int cc = lane; cc < nc; cc += 32) {
+    const int cd = c0 + cc, ic = cd / nfJ, jd = cd - ic * nfJ;
+    double s = 0.0;
+    for (int ab = 0; ab < nA; ++ab) {
+      const int p = ab / nfQ, q = ab - p * nfQ;
+      s = fma(O[ab * nc + cc], PT[(size_t)(fP + p) * N + fQ + q], s);
+    }
+    atomicAdd(a.b.J + (size_t)(fI + ic) * N + fJ + jd, s2 * s);
+  }
+  for (int ab = lane; ab < nA; ab += 32) {
+    const int p = ab / nfQ, q = ab - p * nfQ;
+    double s = 0.0;
+    for (int cc = 0; cc < nc; ++cc) {
+      const int cd = c0 + cc, ic = cd / nfJ, jd = cd - ic * nfJ;
+      s = fma(O[ab * nc + cc], PT[(size_t)(fI + ic) * N + fJ + jd], s);
+    }
+    atomicAdd(a.b.J + (size_t)(fP + p) * N + fQ + q, s2 * s);
+  }
+  const int i0 = c0 / nfJ, i1 = (c0 + nc - 1) / nfJ, ni = i1 - i0 + 1;   // ket rows in the chunk
+  for (int ks = 0; ks < (a.b.uhf ? 2 : 1); ++ks) {
+    const double* __restrict__ D = ks ? a.b.PB : a.b.PA;
+    double* K = ks ? a.b.KB : a.b.KA;
+    // K[p][i] (x = p, y = q) and K[q][i] (x = q, y = p): sums over y and the chunk's j
+    for (int e = lane; e < (nfP + nfQ) * ni; e += 32) {
+      const bool onP = e < nfP * ni;
+      const int e2 = onP ? e : e - nfP * ni;
+      const int x = e2 / ni, ic = i0 + (e2 - (e2 / ni) * ni);
+      const int jlo = max(0, c0 - ic * nfJ), jhi = min(nfJ, c0 + nc - ic * nfJ);
+      const int ny = onP ? nfQ : nfP;
+      double s = 0.0;
+      for (int y = 0; y < ny; ++y) {
+        const int ab = onP ? x * nfQ + y : y * nfQ + x;
+        const int fy = onP ? fQ + y : fP + y;
+        for (int jd = jlo; jd < jhi; ++jd) s = fma(O[ab * nc + ic * nfJ + jd - c0], D[(size_t)fy * N + fJ + jd], s);
+      }
+      atomicAdd(K + (size_t)((onP ? fP : fQ) + x) * N + fI + ic, deg * s);
+    }
+    // K[p][j] and K[q][j]: sums over y and the chunk's i
+    for (int e = lane; e < (nfP + nfQ) * nfJ; e += 32) {
+      const bool onP = e < nfP * nfJ;
+      const int e2 = onP ? e : e - nfP * nfJ;
+      const int x = e2 / nfJ, jd = e2 - x * nfJ;
+      const int ny = onP ? nfQ : nfP;
+      double s = 0.0;
+      for (int y = 0; y < ny; ++y) {
+        const int ab = onP ? x * nfQ + y : y * nfQ + x;
+        const int fy = onP ? fQ + y : fP + y;
+        for (int ic = i0; ic <= i1; ++ic) {
+          const int cd = ic * nfJ + jd;
+          if (cd < c0 || cd >= c0 + nc) continue;
+          s = fma(O[ab * nc + cd - c0], D[(size_t)fy * N + fI + ic], s);
+        }
+      }
+      atomicAdd(K + (size_t)((onP ? fP : fQ) + x) * N + fJ + jd, deg * s);
+    }
+  }
+}
+
+// Largest |O - monopole value| over a chunk (multipole-mode error measurement).
+__device__ double gen_mpole_err(const GenArgs& a, const GenPairRec& A, const GenPairRec& B, const double* O, int c0,
+                                int nc, int lane) {
+  const int nfQ = A.nfQ, nfJ = B.nfQ, nA = A.nfP * nfQ;
+  double e = 0.0;
+  for (int x = lane; x < nA * nc; x += 32) {
+    const int ab = x / nc, cc = x - ab * nc, cd = c0 + cc;
+    const int pp = ab / nfQ, ic = cd / nfJ;
+    const double m = sqb::mpole_value(a.b.mpole, a.b.nbf, A.fP + pp, A.fQ + ab - pp * nfQ, B.fP + ic, B.fQ + cd - ic * nfJ);
+    e = fmax(e, fabs(O[x] - m));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(0xffffffffu, e, o));
+  return e;
+}
+
+// One shell quartet (A|B) by one warp; W is the warp's shared-memory region.  npq counts the
+// primitive quartets that pass the prefactor cut (first chunk only).  Multipole mode: mpq
+// substitutes the monopole values for the integrals (no primitive work), erx >= 0 records the
+// largest monopole error of the exact block in the bank's scratch.
+__device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPairRec& B, double deg, double* W, int lane,
+                            unsigned long long& npq, bool mpq, int erx) {
+  double* base = W;
+  double* R0 = base + 16;
+  double* R1 = R0 + kGenR;
+  double* Eb = R1 + kGenR;
+  double* Ek = Eb + kGenE;
+  double* G = Ek + kGenE;
+  const int nfQ = A.nfQ, nfJ = B.nfQ;
+  const int nA = A.nfP * nfQ, nB = B.nfP * nfJ;
+  const int LA = A.lP + A.lQ, LB = B.lP + B.lQ, L = LA + LB;
+  const int nHA = (LA + 1) * (LA + 2) * (LA + 3) / 6;
+  const int ncm = min(nB, kGenGO / (nA + nHA));
+  double* O = G + nHA * ncm;
+  for (int c0 = 0; c0 < nB; c0 += ncm) {
+    const int nc = min(ncm, nB - c0);
+    if (mpq) {
+      for (int e = lane; e < nA * nc; e += 32) {
+        const int ab = e / nc, cd = c0 + e - (e / nc) * nc;
+        const int pp = ab / nfQ, ic = cd / nfJ;
+        O[e] = sqb::mpole_value(a.b.mpole, a.b.nbf, A.fP + pp, A.fQ + ab - pp * nfQ, B.fP + ic, B.fQ + cd - ic * nfJ);
+      }
+      __syncwarp();
+      gen_digest(a, A, B, deg, O, c0, nc, lane);
+      __syncwarp();
+      continue;
+    }
+    for (int e = lane; e < nA * nc; e += 32) O[e] = 0.0;
+    for (int i = 0; i < A.nprim; ++i) {
+      const double* pa = a.prims + (size_t)(A.poff + i) * kGenPrimStride;
+      const double p = pa[0], Px = pa[1], Py = pa[2], Pz = pa[3], kpa = pa[4];
+      const int ia = (int)pa[14], ib = (int)pa[15];
+      __syncwarp();                                  // the previous O step is done with Eb and G
+      if (lane < 3) gen_e1d(p, pa[5 + lane], pa[8 + lane], A.lP, A.lQ, Eb + lane * kGenE1);
+      for (int e = lane; e < nHA * nc; e += 32) G[e] = 0.0;
+      bool any = false;
+      for (int j = 0; j < B.nprim; ++j) {
+        const double* pb = a.prims + (size_t)(B.poff + j) * kGenPrimStride;
+        const double q = pb[0], kpb = pb[4];
+        const double pq = p + q, rs = rsqrt(pq);
+        if (TWO_PI_2_5 * kpa * kpb * rs < PRIM_CUTOFF) continue;
+        any = true;
+        if (c0 == 0) ++npq;
+        const double alpha = p * q * (rs * rs);
+        const double X = Px - pb[1], Y = Py - pb[2], Z = Pz - pb[3];
+        const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));
+        __syncwarp();                                // the previous G step is done with Ek and R
+        if (lane < 3) gen_e1d(q, pb[5 + lane], pb[8 + lane], B.lP, B.lQ, Ek + lane * kGenE1);
+        gen_seeds(L, alpha, rs, T, a.boys, base, lane);
+        __syncwarp();
+        const double* R = gen_rtab(L, X, Y, Z, base, R0, R1, lane);
+        const int ja = (int)pb[14], jb = (int)pb[15];
+        for (int e = lane; e < nHA * nc; e += 32) {
+          const int h = e / nc, cc = e - h * nc;
+          const unsigned tv = g_tuv.v[h];
+          const int t = tv & 255, u = (tv >> 8) & 255, v = tv >> 16;
+          const int cd = c0 + cc, ic = cd / nfJ, jd = cd - ic * nfJ;
+          const int fI = B.fP + ic, fJ = B.fQ + jd;
+          const int cx = a.lmn[3 * fI], cy = a.lmn[3 * fI + 1], cz = a.lmn[3 * fI + 2];
+          const int dx = a.lmn[3 * fJ], dy = a.lmn[3 * fJ + 1], dz = a.lmn[3 * fJ + 2];
+          const double s = ket_sum(Ek + (cx * 4 + dx) * 7, Ek + kGenE1 + (cy * 4 + dy) * 7,
+                                   Ek + 2 * kGenE1 + (cz * 4 + dz) * 7, cx + dx, cy + dy, cz + dz, t, u, v, R);
+          G[e] = fma(gcoef(a, fI, ja) * gcoef(a, fJ, jb) * kpb, s, G[e]);
+        }
+      }
+      __syncwarp();
+      if (!any) continue;
+      for (int e = lane; e < nA * nc; e += 32) {
+        const int ab = e / nc, cc = e - ab * nc;
+        const int pp = ab / nfQ, qq = ab - pp * nfQ;
+        const int fP = A.fP + pp, fQ = A.fQ + qq;
+        const int ax = a.lmn[3 * fP], ay = a.lmn[3 * fP + 1], az = a.lmn[3 * fP + 2];
+        const int bx = a.lmn[3 * fQ], by = a.lmn[3 * fQ + 1], bz = a.lmn[3 * fQ + 2];
+        const double* ex = Eb + (ax * 4 + bx) * 7;
+        const double* ey = Eb + kGenE1 + (ay * 4 + by) * 7;
+        const double* ez = Eb + 2 * kGenE1 + (az * 4 + bz) * 7;
+        double s = 0.0;
+        for (int t = 0; t <= ax + bx; ++t)
+          for (int u = 0; u <= ay + by; ++u) {
+            double sz = 0.0;
+            for (int v = 0; v <= az + bz; ++v) sz = fma(ez[v], G[gtet(t, u, v) * nc + cc], sz);
+            s = fma(ex[t] * ey[u], sz, s);
+          }
+        O[e] = fma(gcoef(a, fP, ia) * gcoef(a, fQ, ib) * kpa, s, O[e]);
+      }
+    }
+    __syncwarp();
+    if (erx >= 0) {
+      const double e = gen_mpole_err(a, A, B, O, c0, nc, lane);
+      if (lane == 0) atomicMax(a.b.erscr + erx, (unsigned long long)__double_as_longlong(e) | (1ull << 63));
+    }
+    gen_digest(a, A, B, deg, O, c0, nc, lane);
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(32 * kGenWarps) k_jk_gen(const GenArgs a, const GenItem* __restrict__ items) {
+  extern __shared__ double gsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* W = gsm + warp * kGenWarpDoubles;
+  const GenItem it = items[blockIdx.x];
+  const GenPairRec A = a.pairs[it.bra];
+  unsigned long long nq = 0, npq = 0;
+  for (int kk = warp; kk < it.cnt; kk += kGenWarps) {
+    const int kb = it.k0 + kk;
+    const GenPairRec B = a.pairs[kb];
+    if (B.gen && kb < it.bra) continue;              // two generic pairs: taken once, from the later one
+    const double r = A.schwarz * B.schwarz;
+    bool ok = !(r < a.b.cut_outer) && !(r < a.b.cut_fixed);
+    // multipole mode: the quartet's bank slot and stored exponent; a known exponent below the
+    // cache bound makes it a substitution candidate (the class kernels' rule)
+    int erx = -1, erexp = sqb::ERR_UNKNOWN;
+    if (ok && a.b.erbank && it.er >= 0) { erx = it.er + kb; erexp = a.b.erbank[erx]; }
+    const bool mpc = erexp != sqb::ERR_UNKNOWN && r < a.b.mp_rmax;
+    bool mpq = false;
+    if (ok && (r < a.b.dscreen_rmax || mpc)) {
+      // density screen in the reference's orientation, pair(P,Q) >= pair(I,J)
+      const bool bf = (A.P > B.P) || (A.P == B.P && A.Q >= B.Q);
+      const int P = bf ? A.P : B.P, Q = bf ? A.Q : B.Q, I = bf ? B.P : A.P, J = bf ? B.Q : A.Q;
+      const double* PM = a.b.PM;
+      const int ns = a.b.ns;
+      const double mp = PM[P * ns + Q] + PM[I * ns + J] + PM[P * ns + I] + PM[P * ns + J] + PM[Q * ns + I] + PM[Q * ns + J];
+      if (r < a.b.dscreen_rmax) ok = !(r * mp < a.b.cut_fixed);
+      if (ok && mpc) mpq = a.b.pow15[erexp - sqb::ERR_MIN] * mp < a.b.cut_fixed;
+    }
+    if (!ok) continue;
+    const double deg = (A.P == A.Q ? 0.5 : 1.0) * (B.P == B.Q ? 0.5 : 1.0) * (kb == it.bra ? 0.5 : 1.0);
+    ++nq;
+    gen_quartet(a, A, B, deg, W, lane, npq, mpq, erexp == sqb::ERR_UNKNOWN ? erx : -1);
+  }
+  if (lane == 0) {
+    if (nq) atomicAdd(a.counters, nq);
+    if (npq) atomicAdd(a.counters + 1, npq);
+  }
+}
+
+// sqrt|(ab|ab)| for every function pair of the generic pairs: one warp per pair, lanes over
+// its function pairs, every primitive quartet of (A|A) (no prefactor cut, as create_Schwarz,
+// reference src/matrix.c:389-440, evaluates the full contracted integral).
+__global__ void __launch_bounds__(32 * kGenWarps) k_gen_schwarz(const GenArgs a, const int* __restrict__ gidx, int ngen,
+                                                               int nbf, double* __restrict__ S) {
+  extern __shared__ double gsm[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * kGenWarps + warp;
+  if (w >= ngen) return;                             // whole warps leave together
+  double* base = gsm + warp * kGenWarpDoubles;
+  double* R0 = base + 16;
+  double* R1 = R0 + kGenR;
+  double* Eb = R1 + kGenR;
+  double* Ek = Eb + kGenE;
+  double* acc = Ek + kGenE;
+  const GenPairRec A = a.pairs[gidx[w]];
+  const int nfQ = A.nfQ, nA = A.nfP * nfQ, L = 2 * (A.lP + A.lQ);
+  for (int e = lane; e < nA; e += 32) acc[e] = 0.0;
+  for (int i = 0; i < A.nprim; ++i) {
+    const double* pi = a.prims + (size_t)(A.poff + i) * kGenPrimStride;
+    const double p = pi[0], kpi = pi[4];
+    const int ia = (int)pi[14], ib = (int)pi[15];
+    __syncwarp();
+    if (lane < 3) gen_e1d(p, pi[5 + lane], pi[8 + lane], A.lP, A.lQ, Eb + lane * kGenE1);
+    for (int j = 0; j < A.nprim; ++j) {
+      const double* pj = a.prims + (size_t)(A.poff + j) * kGenPrimStride;
+      const double q = pj[0], kpj = pj[4];
+      const double pq = p + q, rs = rsqrt(pq), alpha = p * q * (rs * rs);
+      const double X = pi[1] - pj[1], Y = pi[2] - pj[2], Z = pi[3] - pj[3];
+      const double T = alpha * (X * X + Y * Y + Z * Z);
+      const int ja = (int)pj[14], jb = (int)pj[15];
+      __syncwarp();
+      if (lane < 3) gen_e1d(q, pj[5 + lane], pj[8 + lane], A.lP, A.lQ, Ek + lane * kGenE1);
+      gen_seeds(L, alpha, rs, T, a.boys, base, lane);
+      __syncwarp();
+      const double* R = gen_rtab(L, X, Y, Z, base, R0, R1, lane);
+      for (int e = lane; e < nA; e += 32) {
+        const int pp = e / nfQ, qq = e - pp * nfQ;
+        const int fP = A.fP + pp, fQ = A.fQ + qq;
+        const int ax = a.lmn[3 * fP], ay = a.lmn[3 * fP + 1], az = a.lmn[3 * fP + 2];
+        const int bx = a.lmn[3 * fQ], by = a.lmn[3 * fQ + 1], bz = a.lmn[3 * fQ + 2];
+        const int nx = ax + bx, ny = ay + by, nz = az + bz;
+        const double* kx = Ek + (ax * 4 + bx) * 7;
+        const double* ky = Ek + kGenE1 + (ay * 4 + by) * 7;
+        const double* kz = Ek + 2 * kGenE1 + (az * 4 + bz) * 7;
+        const double* ex = Eb + (ax * 4 + bx) * 7;
+        const double* ey = Eb + kGenE1 + (ay * 4 + by) * 7;
+        const double* ez = Eb + 2 * kGenE1 + (az * 4 + bz) * 7;
+        double s = 0.0;
+        for (int t = 0; t <= nx; ++t)
+          for (int u = 0; u <= ny; ++u)
+            for (int v = 0; v <= nz; ++v) s = fma(ex[t] * ey[u] * ez[v], ket_sum(kx, ky, kz, nx, ny, nz, t, u, v, R), s);
+        const double wi = gcoef(a, fP, ia) * gcoef(a, fQ, ib) * kpi;
+        const double wj = gcoef(a, fP, ja) * gcoef(a, fQ, jb) * kpj;
+        acc[e] = fma(wi * wj, s, acc[e]);
+      }
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < nA; e += 32) {
+    const int pp = e / nfQ, qq = e - pp * nfQ;
+    const double v = sqrt(fabs(acc[e]));
+    S[(size_t)(A.fP + pp) * nbf + A.fQ + qq] = v;
+    S[(size_t)(A.fQ + qq) * nbf + A.fP + pp] = v;
+  }
+}
+
+GenArgs make_args(const sqb::GenPath& g) {
+  GenArgs a;
+  memset(&a, 0, sizeof(a));
+  a.pairs = g.d_pairs;
+  a.prims = g.d_prims;
+  a.lmn = g.d_lmn;
+  a.foff = g.d_foff;
+  a.ncoef = g.d_ncoef;
+  a.boys = g.d_boys;
+  a.counters = g.d_counters;
+  return a;
+}
+
+int set_smem() {
+  static int done = 0;
+  static cudaError_t err = cudaSuccess;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!(done & (1 << (dev & 31)))) {
+    err = cudaFuncSetAttribute(k_jk_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmem);
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_gen_schwarz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmem);
+    if (err != cudaSuccess) return sqb::set_error(SQB200_ECUDA, std::string("generic kernels: ") + cudaGetErrorString(err));
+    done |= 1 << (dev & 31);
+  }
+  return SQB200_OK;
+}
+
+}  // namespace
+
+namespace sqb {
+
+void gen_build_pairs(GenPath& g, const std::vector<GenShell>& sh, const double* schwarz, int nbf) {
+  g.pairs.clear();
+  g.prims.clear();
+  g.gen_idx.clear();
+  const int ns = (int)sh.size();
+  struct Tmp { double s; int P, Q; };
+  std::vector<Tmp> all;
+  all.reserve((size_t)ns * (ns + 1) / 2);
+  for (int P = 0; P < ns; ++P)
+    for (int Q = 0; Q <= P; ++Q) {
+      double r = 0.0;
+      for (int p = 0; p < sh[P].nfunc; ++p)
+        for (int q = 0; q < sh[Q].nfunc; ++q) r = std::max(r, schwarz[(size_t)(sh[P].first + p) * nbf + sh[Q].first + q]);
+      all.push_back({r, P, Q});
+    }
+  std::stable_sort(all.begin(), all.end(), [](const Tmp& x, const Tmp& y) { return x.s > y.s; });
+  for (const Tmp& t : all) {
+    const GenShell& A = sh[t.P];
+    const GenShell& B = sh[t.Q];
+    GenPairRec rec;
+    rec.P = t.P; rec.Q = t.Q; rec.fP = A.first; rec.fQ = B.first;
+    rec.nfP = A.nfunc; rec.nfQ = B.nfunc; rec.lP = A.lmax; rec.lQ = B.lmax;
+    rec.nprim = A.nprim * B.nprim;
+    rec.poff = (int)(g.prims.size() / kGenPrimStride);
+    rec.gen = (A.gen || B.gen) ? 1 : 0;
+    rec.pad_ = 0;
+    rec.schwarz = t.s;
+    // primitive data as the class kernels' pair records compute it (same expressions, so the
+    // prefactor cut decides alike)
+    const double ab2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
+    for (int i = 0; i < A.nprim; ++i)
+      for (int j = 0; j < B.nprim; ++j) {
+        const double a = A.exps[i], b = B.exps[j], p = a + b;
+        const double Px = (a * A.x + b * B.x) / p, Py = (a * A.y + b * B.y) / p, Pz = (a * A.z + b * B.z) / p;
+        const double kp = std::exp(-a * b * ab2 / p) / p;
+        const double f[kGenPrimStride] = {p, Px, Py, Pz, kp, Px - A.x, Py - A.y, Pz - A.z, Px - B.x, Py - B.y,
+                                          Pz - B.z, 0.0, 0.0, 0.0, (double)i, (double)j};
+        g.prims.insert(g.prims.end(), f, f + kGenPrimStride);
+      }
+    if (rec.gen) g.gen_idx.push_back((int)g.pairs.size());
+    g.pairs.push_back(rec);
+  }
+}
+
+int gen_upload(GenPath& g, int nbf, const int* nprim, const int* lmn, const double* ncoefs, cudaStream_t st) {
+  std::vector<int> foff(nbf);
+  size_t tot = 0;
+  for (int i = 0; i < nbf; ++i) { foff[i] = (int)tot; tot += nprim[i]; }
+  const std::vector<double> tab = boys_table(kGenBoysCols);
+  struct Slot { void** dst; size_t bytes; const void* src; };
+  const Slot slots[] = {
+      {(void**)&g.d_pairs, g.pairs.size() * sizeof(GenPairRec), g.pairs.data()},
+      {(void**)&g.d_prims, g.prims.size() * sizeof(double), g.prims.data()},
+      {(void**)&g.d_gen_idx, g.gen_idx.size() * sizeof(int), g.gen_idx.data()},
+      {(void**)&g.d_lmn, (size_t)nbf * 3 * sizeof(int), lmn},
+      {(void**)&g.d_foff, (size_t)nbf * sizeof(int), foff.data()},
+      {(void**)&g.d_ncoef, tot * sizeof(double), ncoefs},
+      {(void**)&g.d_boys, tab.size() * sizeof(double), tab.data()},
+      {(void**)&g.d_counters, 2 * sizeof(unsigned long long), nullptr},
+  };
+  auto rnd = [](size_t b) { return (std::max<size_t>(b, 1) + 255) / 256 * 256; };
+  size_t bytes = 0;
+  for (const Slot& s : slots) bytes += rnd(s.bytes);
+  if (g.d_base && g.bytes != bytes) gen_free(g);
+  if (!g.d_base) {
+    const cudaError_t e = cudaMalloc(&g.d_base, bytes);
+    if (e != cudaSuccess) {
+      g.d_base = nullptr;
+      return set_error(SQB200_ENOMEM, std::string("cudaMalloc (generic path): ") + cudaGetErrorString(e));
+    }
+    g.bytes = bytes;
+  }
+  std::vector<char> img(bytes, 0);
+  size_t o = 0;
+  for (const Slot& s : slots) {
+    *s.dst = (char*)g.d_base + o;
+    if (s.src && s.bytes) memcpy(img.data() + o, s.src, s.bytes);
+    o += rnd(s.bytes);
+  }
+  cudaError_t e = cudaMemcpyAsync(g.d_base, img.data(), bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return set_error(SQB200_ECUDA, std::string("generic path upload: ") + cudaGetErrorString(e));
+  return SQB200_OK;
+}
+
+int gen_schwarz(const GenPath& g, int nbf, double* S, cudaStream_t st) {
+  if (g.gen_idx.empty()) return SQB200_OK;
+  int rc = set_smem();
+  if (rc) return rc;
+  const int ngen = (int)g.gen_idx.size();
+  k_gen_schwarz<<<(ngen + kGenWarps - 1) / kGenWarps, 32 * kGenWarps, kGenSmem, st>>>(make_args(g), g.d_gen_idx, ngen,
+                                                                                     nbf, S);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(SQB200_ECUDA, std::string("k_gen_schwarz: ") + cudaGetErrorString(e));
+  return SQB200_OK;
+}
+
+void gen_items(const GenPath& g, double outer, double fixed, std::vector<GenItem>& items, double& cost,
+               long long* er_run) {
+  const double cut = std::max(outer, fixed);
+  const int np = (int)g.pairs.size();
+  // kets with schwarz >= c / S(A) (less a relative 1e-12 that the kernel's exact test takes
+  // back): a prefix of the sorted list
+  auto prefix = [&](double c, double sa) {
+    const double thr = c / sa * (1.0 - 1e-12);
+    int lo = 0, hi = np;
+    while (lo < hi) {
+      const int mid = (lo + hi) / 2;
+      if (g.pairs[mid].schwarz >= thr) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+  };
+  for (int a : g.gen_idx) {
+    const GenPairRec& A = g.pairs[a];
+    if (!(A.schwarz > 0.0)) continue;
+    const int lo = prefix(cut, A.schwarz);
+    int er = -1;
+    if (er_run) {   // slots for the outer cutoff's survivors, so the layout does not depend on `fixed`
+      er = (int)*er_run;
+      *er_run += prefix(outer, A.schwarz);
+    }
+    for (int k0 = 0; k0 < lo; k0 += kGenKets) items.push_back({a, k0, std::min(kGenKets, lo - k0), er});
+    cost += (double)lo * A.nprim * A.nfP * A.nfQ * 200.0;
+  }
+}
+
+int gen_launch(const GenPath& g, const GenItem* d_items, int nitems, const GenBuild& b, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(g.d_counters, 0, 2 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return set_error(SQB200_ECUDA, std::string("generic counters: ") + cudaGetErrorString(e));
+  if (nitems <= 0) return SQB200_OK;
+  int rc = set_smem();
+  if (rc) return rc;
+  GenArgs a = make_args(g);
+  a.b = b;
+  k_jk_gen<<<nitems, 32 * kGenWarps, kGenSmem, st>>>(a, d_items);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(SQB200_ECUDA, std::string("k_jk_gen: ") + cudaGetErrorString(e));
+  return SQB200_OK;
+}
+
+void gen_free(GenPath& g) {
+  if (g.d_base) cudaFree(g.d_base);
+  g.d_base = nullptr;
+  g.bytes = 0;
+  g.d_pairs = nullptr;
+  g.d_prims = nullptr;
+  g.d_gen_idx = nullptr;
+  g.d_lmn = nullptr;
+  g.d_foff = nullptr;
+  g.d_ncoef = nullptr;
+  g.d_boys = nullptr;
+  g.d_counters = nullptr;
+}
+
+}  // namespace sqb

@@ -1,6 +1,7 @@
 """Extract Gaussian basis-set tables from GAMESS-US format files into basis_sets.json.
 
-The published Pople basis sets (STO-3G, 3-21G, 6-31G, 6-31G*) ship with the reference as
+The published Pople basis sets (STO-3G, 3-21G, 6-31G, 6-31G*) and the DZP and QZP sets of the
+Jorge group (with f shells: QZP on every heavy atom, DZP from potassium on) ship with the reference as
 GAMESS-format text (basis/*.txt; parsed by read_GAMESS_BasisSet, src/basis.c:316-514).  The
 GPU host has no reference tree, so the tables the workloads need are converted once into a
 JSON data file that travels with this package.  Only exponents and contraction coefficients
@@ -13,7 +14,7 @@ import os
 import sys
 
 FILES = {"sto3g": "sto3g.txt", "321g": "321g.txt", "631g": "631g.txt",
-         "631g_star": "631g_star.txt"}
+         "631g_star": "631g_star.txt", "dzp": "DZP.txt", "qzp_gh": "QZP-gh.txt"}
 
 ELEMENTS = ["HYDROGEN", "HELIUM", "LITHIUM", "BERYLLIUM", "BORON", "CARBON", "NITROGEN",
             "OXYGEN", "FLUORINE", "NEON", "SODIUM", "MAGNESIUM", "ALUMINUM", "SILICON",

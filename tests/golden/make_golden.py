@@ -15,6 +15,7 @@ Usage:  make -C oracle && python tests/golden/make_golden.py
         python tests/golden/make_golden.py --oneint   (add S, T, V to existing fixtures only)
         python tests/golden/make_golden.py --iters    (add the reference's SCF iteration count)
         python tests/golden/make_golden.py --forces   (add the reference's forces, uhf_force)
+        python tests/golden/make_golden.py --fshells  (the f-shell cases, FSHELL_CASES)
 """
 import os
 import subprocess
@@ -61,6 +62,13 @@ CASES = [
     ("oh_321g_uhf", hydroxyl, "321g", ()),
     ("h2co_631gs", formaldehyde, "631g_star", ()),
     ("benzene_631gs", M.benzene, "631g_star", ()),
+]
+
+# bases with f shells (QZP: two f shells on every heavy atom, one on hydrogen), for the
+# generic quartet path; made by `--fshells`
+FSHELL_CASES = [
+    ("water_qzp", M.water, "QZP-gh", ()),
+    ("oh_qzp_uhf", hydroxyl, "QZP-gh", ()),
 ]
 
 
@@ -132,8 +140,8 @@ def add_forces():
         print(name, "reference forces", F.tolist())
 
 
-def main():
-    for name, geom, bas, opts in CASES:
+def main(cases=CASES):
+    for name, geom, bas, opts in cases:
         atoms = geom()
         with tempfile.TemporaryDirectory() as d:
             xyz = os.path.join(d, "m.xyz")
@@ -165,5 +173,7 @@ if __name__ == "__main__":
         add_scf_iters()
     elif "--forces" in sys.argv[1:]:
         add_forces()
+    elif "--fshells" in sys.argv[1:]:
+        main(FSHELL_CASES)
     else:
         main()

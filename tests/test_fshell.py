@@ -1,0 +1,242 @@
+"""Bases with f shells: the generic quartet path (csrc/jk_generic.cu) beside the generated class
+kernels.
+
+The reference reads f shells from GAMESS basis files (read_GAMESS_BasisSet, src/basis.c:488-499)
+and types a ten-function shell TYPEF (genGTOShell, src/matrix.c:2527-2535); its QZP set gives
+every heavy atom two f shells and hydrogen one.  The fixtures water_qzp (RHF, 126 functions)
+and oh_qzp_uhf (UHF, 91) hold the reference's own basis arrays, Schwarz matrix, converged
+densities, one-electron matrices and J/K builds (tests/golden/make_golden.py --fshells).
+
+CPU: the package's basis builder and the oracle port against those fixtures.
+GPU: J/K, device Schwarz, one-electron matrices and whole SCF energies against the reference,
+quartet counts against the port, at the plain-FP64 bars (1e-10 on J/K, 1e-8 Eh on energies)."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden, golden_basis, load_oracle, load_sqb200
+
+TOL = 1e-10
+FCASES = ["water_qzp", "oh_qzp_uhf"]
+port = load_oracle()
+SQREF_GPU = os.path.join(ROOT, "oracle", "_ref", "sqref_b200")
+
+
+def _atoms(g):
+    return [(int(a[0]), float(a[1]), float(a[2]), float(a[3])) for a in g["atoms"]]
+
+
+@pytest.mark.parametrize("case", FCASES)
+def test_basis_builder_matches_reference_with_f_shells(case):
+    sqb = load_sqb200()
+    g = golden(case)
+    b = sqb.basis.build_basis(sqb.molecules.to_bohr(_atoms(g)), str(g["basis"]))
+    assert np.array_equal(b.nprim, g["nprim"]) and np.array_equal(b.lmn, g["lmn"])
+    assert np.array_equal(b.exps, g["exps"]) and np.array_equal(b.coefs, g["coefs"])
+    assert np.abs(b.norms - g["norms"]).max() <= 1e-15 * np.abs(g["norms"]).max()
+    assert int((b.lmn.sum(axis=1) == 3).sum()) > 0          # the case has f functions
+
+
+def test_port_matches_reference_with_f_shells():
+    """The oracle port (which handles f shells like the reference, by THO) against the
+    reference's own J/K, both screening modes, and its Schwarz matrix."""
+    g = golden("oh_qzp_uhf")
+    b = golden_basis(g)
+    np.testing.assert_allclose(port.schwarz(b), g["schwarz"], rtol=1e-12, atol=1e-14)
+    for mode in ("mem", "dir"):
+        rmax = port.mem_cutoff(b, g["schwarz"], 1e-10, 250 if mode == "mem" else 0)
+        JT, KA, KB, _ = port.jk_build(b, g["schwarz"], g["PA"], g["PB"], restricted=False, scf_cutoff=1e-10,
+                                      dscreen_rmax=rmax)
+        for k, M in (("JT", JT), ("KA", KA), ("KB", KB)):
+            assert np.abs(M - g[k + "_" + mode]).max() <= TOL, (mode, k)
+
+
+def _engine(g, schwarz=True):
+    sqb = load_sqb200()
+    return sqb.JKEngine(golden_basis(g), schwarz=g["schwarz"] if schwarz else None)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", FCASES)
+@pytest.mark.parametrize("mode", ["mem", "dir"])
+def test_fshell_jk_matches_reference(case, mode):
+    g = golden(case)
+    b = golden_basis(g)
+    eng = _engine(g)
+    restricted = bool(g["restricted"])
+    rmax = eng.mem_cutoff(1e-10, 250 if mode == "mem" else 0)
+    assert rmax == port.mem_cutoff(b, g["schwarz"], 1e-10, 250 if mode == "mem" else 0)
+    PB = None if restricted else g["PB"]
+    JT, KA, KB = eng.build(g["PA"], PB, restricted=restricted, scf_cutoff=1e-10, dscreen_rmax=rmax)
+    for k, M in (("JT", JT), ("KA", KA), ("KB", KB)):
+        err = np.abs(M - g[k + "_" + mode]).max()
+        assert err <= TOL, (case, mode, k, err)
+        assert np.array_equal(M, M.T), k
+    # the same quartets and primitive quartets as the oracle's pass over every quartet
+    _, _, _, st = port.jk_build(b, g["schwarz"], g["PA"], PB, restricted=restricted, scf_cutoff=1e-10,
+                                dscreen_rmax=rmax)
+    assert eng.stats()["quartets"] == st[1]
+    assert eng.stats()["prim_quartets"] == st[2]
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_fshell_random_density_matches_port():
+    """Arbitrary symmetric densities, restricted and unrestricted, both screening modes."""
+    g = golden("oh_qzp_uhf")
+    b = golden_basis(g)
+    n = b.nbf
+    rng = np.random.default_rng(11)
+    A = rng.normal(size=(n, n)); A = 0.3 * (A + A.T)
+    B = rng.normal(size=(n, n)); B = 0.3 * (B + B.T)
+    eng = _engine(g)
+    for restricted in (True, False):
+        for rmax in (float("inf"), 0.0):
+            PB = None if restricted else B
+            JT, KA, KB = eng.build(A, PB, restricted=restricted, scf_cutoff=1e-10, dscreen_rmax=rmax)
+            J0, K0, KB0, st = port.jk_build(b, g["schwarz"], A, PB, restricted=restricted, scf_cutoff=1e-10,
+                                            dscreen_rmax=rmax)
+            assert np.abs(JT - J0).max() <= TOL
+            assert np.abs(KA - K0).max() <= TOL
+            assert np.abs(KB - KB0).max() <= TOL
+            assert eng.stats()["quartets"] == st[1]
+            assert eng.stats()["prim_quartets"] == st[2]
+    eng.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", FCASES)
+def test_fshell_device_schwarz_and_oneint_match_reference(case):
+    sqb = load_sqb200()
+    g = golden(case)
+    eng = _engine(g, schwarz=False)             # Schwarz bounds computed on the device
+    np.testing.assert_allclose(eng.schwarz(), g["schwarz"], rtol=1e-12, atol=1e-14)
+    restricted = bool(g["restricted"])
+    JT, KA, _ = eng.build(g["PA"], None if restricted else g["PB"], restricted=restricted, scf_cutoff=1e-10)
+    assert np.abs(JT - g["JT_dir"]).max() <= TOL
+    assert np.abs(KA - g["KA_dir"]).max() <= TOL
+    atoms = sqb.molecules.to_bohr(_atoms(g))
+    S, T, V = eng.oneint([a[0] for a in atoms], [a[1:] for a in atoms])
+    eng.close()
+    assert np.abs(S - g["S"]).max() <= 1e-12
+    assert np.abs(T - g["T"]).max() <= 1e-11
+    assert np.abs(V - g["V"]).max() <= 1e-10 * max(1.0, np.abs(g["V"]).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", FCASES)
+def test_fshell_device_scf_energy(case):
+    sqb = load_sqb200()
+    g = golden(case)
+    job = sqb.scf.SCFJob(_atoms(g), str(g["basis"]), restricted=bool(g["restricted"]))
+    e = job.run()
+    iters = job.iters
+    job.close()
+    assert job.converged
+    assert abs(e - float(g["energy"])) <= 1e-8, (case, e, float(g["energy"]))
+    assert abs(iters - int(g["scf_iters"])) <= 1
+
+
+def _inputs(d, g):
+    """The molecule and the basis text (written by the package) for a run of the reference."""
+    sqb = load_sqb200()
+    xyz = os.path.join(d, "m.xyz")
+    with open(xyz, "w") as f:
+        f.write(sqb.molecules.xyz_text(_atoms(g)))
+    bas = os.path.join(d, "basis.txt")
+    with open(bas, "w") as f:
+        f.write(sqb.basis.gamess_text(str(g["basis"]), [int(a[0]) for a in g["atoms"]]))
+    return xyz, bas
+
+
+def _dropin(binary, g, opts, env=None):
+    with tempfile.TemporaryDirectory() as d:
+        xyz, bas = _inputs(d, g)
+        r = subprocess.run([binary, "scf", xyz, bas, "-"] + list(opts), capture_output=True, text=True, timeout=900,
+                           env=None if env is None else dict(os.environ, **env))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    res = [line for line in r.stderr.splitlines() if line.startswith("RESULT")]
+    return float(dict(kv.split("=") for kv in res[-1].split()[1:])["energy"])
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(SQREF_GPU), reason="oracle/_ref/sqref_b200 not built")
+@pytest.mark.parametrize("case", FCASES)
+def test_fshell_dropin_scf_energy_matches_reference(case):
+    """The reference program relinked onto the GPU build, 1STEP schedule."""
+    g = golden(case)
+    e = _dropin(SQREF_GPU, g, ["-SCFACC=1STEP", "-SCFCONV=1e-8"])
+    assert abs(e - float(g["energy"])) <= 1e-8, (case, e, float(g["energy"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(SQREF_GPU), reason="oracle/_ref/sqref_b200 not built")
+@pytest.mark.parametrize("maxmem", [None, "0"])
+def test_fshell_dropin_default_schedule_multipole_mode(maxmem):
+    """The reference's default 3STEP schedule with the reference-parity multipole mode
+    (SQB200_MULTIPOLE=1), which the generic path follows too: energies at 1e-8 Eh."""
+    g = golden("oh_qzp_uhf")
+    opts = ["-SCFCONV=1e-8"] + (["-MAXMEM=" + maxmem] if maxmem else [])
+    e_ref = _dropin(port.REF_BIN, g, opts)
+    e_gpu = _dropin(SQREF_GPU, g, opts, env={"SQB200_MULTIPOLE": "1"})
+    assert abs(e_ref - e_gpu) <= 1e-8, (maxmem, e_ref, e_gpu)
+
+
+@pytest.mark.gpu
+def test_fshell_multipole_visits_match_reference():
+    """Reference-parity multipole mode over SCF-like visits (a full density, then shrinking
+    difference densities at tightening cutoffs) against the reference's own sequence."""
+    sqb = load_sqb200()
+    g = golden("oh_qzp_uhf")
+    b = golden_basis(g)
+    rng = np.random.default_rng(5)
+
+    def sym(scale):
+        A = rng.normal(size=(b.nbf, b.nbf)) * scale
+        return A + A.T
+
+    dens = [g["PA"], sym(1e-2), sym(1e-4), sym(1e-6)]
+    cuts = [1e-7, 1e-7, 1e-9, 1e-10]
+    with tempfile.TemporaryDirectory() as d:
+        xyz, bas = _inputs(d, g)
+        ref = port.ref_jkseq(xyz, bas, dens, cuts, scf_cutoff=1e-10, max_mem=0)
+    eng = sqb.JKEngine(b, schwarz=g["schwarz"])
+    memcut = eng.mem_cutoff(cuts[0], 0)
+    eng.set_multipole(True, memcut)
+    for v, (P, c) in enumerate(zip(dens, cuts)):
+        JT, KA, _ = eng.build(P, restricted=True, scf_cutoff=1e-10, fixed_cutoff=c,
+                              dscreen_rmax=memcut if v == 0 else float("inf"))
+        J0, K0 = ref[v]
+        scale = max(np.abs(J0).max(), np.abs(K0).max())
+        for M, M0 in ((JT, J0), (KA, K0)):
+            err = np.abs(M - M0).max()
+            assert err <= TOL and err <= 1e-7 * scale, (v, err, scale)
+    eng.close()
+
+
+@pytest.mark.gpu
+def test_fshell_unsupported_entry_points_fail_loudly():
+    """The allocation-free entry point and batched builds cover s, sp, p and d shells only:
+    with f shells they return SQB200_EUNSUPPORTED instead of a wrong build."""
+    import ctypes
+
+    import torch
+    sqb = load_sqb200()
+    g = golden("oh_qzp_uhf")
+    eng = _engine(g)
+    with pytest.raises(sqb.SQB200Error, match="f shells"):
+        sqb.JKBatch([eng])
+    n = eng.nbf
+    P = torch.zeros((n, n), dtype=torch.float64, device="cuda:0")
+    out = [torch.empty_like(P) for _ in range(3)]
+    lib = sqb.load_library()
+    lib.sqb200_jk_build_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    rc = lib.sqb200_jk_build_noalloc(eng._ctx, P.data_ptr(), P.data_ptr(), 1, 1e-10, 1e-10, 0.0,
+                                     out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), None)
+    assert rc == -2 and b"f shells" in lib.sqb200_last_error()
+    eng.close()
