@@ -741,15 +741,16 @@ void build_pairs(sqb200_jk* c) {
 
 // The generic path's pair data (every shell pair, sorted by the current Schwarz bounds) when
 // the basis has a shell outside the generated classes.
-int setup_generic(sqb200_jk* c, const int* nprim, const int* lmn, const double* ncoefs) {
+int setup_generic(sqb200_jk* c) {
   bool any = false;
   for (const Shell& s : c->shells) any = any || s.gen;
   c->gen.on = any;
   if (!any) return SQB200_OK;
   std::vector<sqb::GenShell> gs;
-  for (const Shell& s : c->shells) gs.push_back({s.first, s.nfunc, s.nprim, s.lmax, s.gen, s.x, s.y, s.z, s.exps});
+  for (const Shell& s : c->shells)
+    gs.push_back({s.first, s.nfunc, s.nprim, s.lmax, s.gen, s.x, s.y, s.z, s.exps, &s.coef[0][0], &s.lmn[0][0]});
   sqb::gen_build_pairs(c->gen, gs, c->schwarz.data(), c->nbf);
-  return sqb::gen_upload(c->gen, c->nbf, nprim, lmn, ncoefs, c->stream);
+  return sqb::gen_upload(c->gen, c->stream);
 }
 
 int compute_schwarz_device(sqb200_jk* c, double* S_host) {
@@ -1434,7 +1435,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
   else c->schwarz.assign((size_t)nbf * nbf, 1.0);   // placeholder until the device pass below
   build_pairs(c);
   rc = upload_pairs(c);
-  if (!rc) rc = setup_generic(c, nprim, lmn, ncoefs);
+  if (!rc) rc = setup_generic(c);
   if (rc) { sqb200_jk_destroy(c); return rc; }
   const size_t nn = (size_t)nbf * nbf;
   std::vector<double> tab = make_boys_table();
@@ -1469,7 +1470,7 @@ int sqb200_jk_create(sqb200_jk** out, int nbf, const int* nprim, const int* lmn,
     if (rc) { sqb200_jk_destroy(c); return rc; }
     build_pairs(c);
     rc = upload_pairs(c);
-    if (!rc) rc = setup_generic(c, nprim, lmn, ncoefs);
+    if (!rc) rc = setup_generic(c);
     if (rc) { sqb200_jk_destroy(c); return rc; }
   }
   // the scratch array of sqb200_jk_build_noalloc: its device address on this device, looked up

@@ -13,10 +13,12 @@
 // of the class kernels (GTO_JK_Matrix_Quartet_Parallel and storeQuartetEE, reference
 // src/matrix.c:3773-3986, 2934-3396), so the two paths add into the same accumulators.
 //
-// Layout: one warp per quartet, two warps per CTA; each warp owns a shared-memory region with
-// the Boys-scaled seeds, two buffers of the R recursion (tetrahedral order t+u+v <= 12), the
-// 1-D Hermite tables of its bra and ket primitive pairs, and G and the contracted block O for
-// a chunk of ket function pairs (chunks when a (ff|ff)-sized block does not fit).
+// Layout: the 1-D Hermite tables and contraction weights of every primitive pair and the
+// component descriptors of every function pair are computed on the host and read through L1;
+// one warp per quartet, two warps per CTA, each warp with a shared-memory region holding the
+// Boys-scaled seeds, two buffers of the R recursion (tetrahedral order t+u+v <= 12), and G and
+// the contracted block O for a chunk of ket function pairs (chunks when a (ff|ff)-sized block
+// does not fit).
 #include "jk_generic.cuh"
 
 #include <algorithm>
@@ -40,13 +42,11 @@ using sqb::kGenPrimStride;
 
 constexpr int kGenBoysCols = 22;                       // orders 0..21: F_12 + 8 Taylor terms
 constexpr int kGenR = 455;                             // tetrahedral entries with t+u+v <= 12
-constexpr int kGenE1 = 4 * 4 * 7;                      // one axis: E^{ij}_t, i, j <= 3, t <= 6
-constexpr int kGenE = 3 * kGenE1;
 constexpr int kGenWarps = 2;                           // warps per CTA
 constexpr int kGenKets = 16;                           // kets per work item
-constexpr int kGenGO = 2048;                           // doubles for G and O of one chunk
-constexpr int kGenWarpDoubles = 16 + 2 * kGenR + 2 * kGenE + kGenGO;
-constexpr size_t kGenSmem = (size_t)kGenWarps * kGenWarpDoubles * sizeof(double);   // 58,336 B
+constexpr int kGenGO = 1024;                           // doubles for G and O of one chunk
+constexpr int kGenWarpDoubles = 16 + 2 * kGenR + kGenGO;
+constexpr size_t kGenSmem = (size_t)kGenWarps * kGenWarpDoubles * sizeof(double);   // 31,200 B
 
 static_assert(sqb::kGenMmax == 12 && (sqb::kGenMmax + 1) * (sqb::kGenMmax + 2) * (sqb::kGenMmax + 3) / 6 == kGenR,
               "R table size");
@@ -72,42 +72,27 @@ __device__ __forceinline__ int gtet(int t, int u, int v) {
 struct GenArgs {
   const GenPairRec* __restrict__ pairs;
   const double* __restrict__ prims;
-  const int* __restrict__ lmn;
-  const int* __restrict__ foff;
-  const double* __restrict__ ncoef;
+  const double* __restrict__ coef;      // per primitive pair: 1-D Hermite tables, then weights
+  const int* __restrict__ desc;         // per pair: component descriptor of each function pair
   const double* __restrict__ boys;
   sqb::GenBuild b;
   unsigned long long* counters;
 };
 
-__device__ __forceinline__ double gcoef(const GenArgs& a, int f, int k) {
-  return __ldg(a.ncoef + __ldg(a.foff + f) + k);
-}
+// A primitive pair's tables in `coef`: axis d, E^{ij}_t at e + d*sz + (i*lq1 + j)*lt + t
+// (i <= lP, j <= lQ, t <= i+j; lq1 = lQ+1, lt = lP+lQ+1, sz = (lP+1) lq1 lt); then the weights
+// c_a c_b exp(-ab|AB|^2/p)/p of its function pairs at e + 3*sz.
+struct EView {
+  const double* e;
+  int lq1, lt, sz;
+  __device__ EView(const double* coef, const double* rec, const GenPairRec& P)
+      : e(coef + (long long)rec[11]), lq1(P.lQ + 1), lt(P.lP + P.lQ + 1), sz((P.lP + 1) * (P.lQ + 1) * (P.lP + P.lQ + 1)) {}
+  __device__ __forceinline__ const double* ax(int d, int i, int j) const { return e + d * sz + (i * lq1 + j) * lt; }
+  __device__ __forceinline__ double w(int ab) const { return __ldg(e + 3 * sz + ab); }
+};
 
-// 1-D Hermite coefficients E^{ij}_t (i <= la, j <= lb) of a primitive pair along one axis into
-// E[(i*4 + j)*7 + t]:  E^{00}_0 = 1,
-// E^{i+1,j}_t = E^{ij}_{t-1}/(2p) + X_PA E^{ij}_t + (t+1) E^{ij}_{t+1}, likewise in j with X_PB.
-__device__ void gen_e1d(double p, double xpa, double xpb, int la, int lb, double* E) {
-  const double h = 0.5 / p;
-  for (int i = 0; i <= la; ++i)
-    for (int j = 0; j <= lb; ++j) {
-      double* e = E + (i * 4 + j) * 7;
-      if (i == 0 && j == 0) {
-        e[0] = 1.0;
-        continue;
-      }
-      const bool up = i > 0;
-      const double* s = up ? E + ((i - 1) * 4 + j) * 7 : E + (i * 4 + j - 1) * 7;
-      const int ls = i + j - 1;                     // highest t of the source
-      const double X = up ? xpa : xpb;
-      for (int t = 0; t <= i + j; ++t) {
-        double v = t <= ls ? X * s[t] : 0.0;
-        if (t > 0) v += h * s[t - 1];
-        if (t + 1 <= ls) v += (t + 1) * s[t + 1];
-        e[t] = v;
-      }
-    }
-}
+// component exponents of a function pair: a_x, b_x, a_y, b_y, a_z, b_z in 2 bits each
+__device__ __forceinline__ int dsc(unsigned d, int k) { return (d >> (2 * k)) & 3; }
 
 // F_n(T) for one order n <= 12: below BOYS_TMAX the 9-term Taylor expansion about the nearest
 // grid point, F_n(T0+d) = sum_k F_{n+k}(T0) (-d)^k / k!, from the table's own column n; above,
@@ -172,19 +157,32 @@ __device__ const double* gen_rtab(int L, double X, double Y, double Z, const dou
   return cur;
 }
 
-// sum_{tau,nu,phi} (-1)^(tau+nu+phi) E_x[tau] E_y[nu] E_z[phi] R_{t+tau,u+nu,v+phi}
-__device__ __forceinline__ double ket_sum(const double* ex, const double* ey, const double* ez, int nx, int ny, int nz,
-                                          int t, int u, int v, const double* R) {
+// sum_{tau,nu,phi} (-1)^(tau+nu+phi) E_x[tau] E_y[nu] E_z[phi] R_{t+tau,u+nu,v+phi}; the
+// tetrahedral index of R steps along phi by increments (n = t+u+v and m = u+v both rise by one)
+__device__ __forceinline__ double ket_sum(const double* __restrict__ ex, const double* __restrict__ ey,
+                                          const double* __restrict__ ez, int nx, int ny, int nz, int t, int u, int v,
+                                          const double* R) {
   double s = 0.0;
-  for (int tau = 0; tau <= nx; ++tau)
+  for (int tau = 0; tau <= nx; ++tau) {
+    const double et = __ldg(ex + tau);
     for (int nu = 0; nu <= ny; ++nu) {
+      const int U = u + nu;
+      int n = t + tau + U + v, m = U + v;
+      int idx = n * (n + 1) * (n + 2) / 6 + m * (m + 1) / 2 + v;
+      int dn = (n + 1) * (n + 2) / 2;                // tet(n+1) - tet(n)
       double sz = 0.0;
       for (int ph = 0; ph <= nz; ++ph) {
-        const double r = R[gtet(t + tau, u + nu, v + ph)] * ez[ph];
-        sz += ((tau + nu + ph) & 1) ? -r : r;
+        const double e = __ldg(ez + ph);
+        sz = fma((ph & 1) ? -e : e, R[idx], sz);
+        idx += dn + m + 2;
+        dn += n + 2;
+        ++n;
+        ++m;
       }
-      s = fma(ex[tau] * ey[nu], sz, s);
+      const double en = __ldg(ey + nu);
+      s = fma(((tau + nu) & 1) ? -et * en : et * en, sz, s);
     }
+  }
   return s;
 }
 
@@ -284,9 +282,7 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
   double* base = W;
   double* R0 = base + 16;
   double* R1 = R0 + kGenR;
-  double* Eb = R1 + kGenR;
-  double* Ek = Eb + kGenE;
-  double* G = Ek + kGenE;
+  double* G = R1 + kGenR;
   const int nfQ = A.nfQ, nfJ = B.nfQ;
   const int nA = A.nfP * nfQ, nB = B.nfP * nfJ;
   const int LA = A.lP + A.lQ, LB = B.lP + B.lQ, L = LA + LB;
@@ -306,13 +302,14 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
       __syncwarp();
       continue;
     }
+    // lane steps through the (row, column) entries of an rows x nc block: 32 = dq*nc + dr
+    const int dq = 32 / nc, dr = 32 - dq * nc;
     for (int e = lane; e < nA * nc; e += 32) O[e] = 0.0;
     for (int i = 0; i < A.nprim; ++i) {
       const double* pa = a.prims + (size_t)(A.poff + i) * kGenPrimStride;
       const double p = pa[0], Px = pa[1], Py = pa[2], Pz = pa[3], kpa = pa[4];
-      const int ia = (int)pa[14], ib = (int)pa[15];
-      __syncwarp();                                  // the previous O step is done with Eb and G
-      if (lane < 3) gen_e1d(p, pa[5 + lane], pa[8 + lane], A.lP, A.lQ, Eb + lane * kGenE1);
+      const EView Ei(a.coef, pa, A);
+      __syncwarp();                                  // the previous O step is done with G
       for (int e = lane; e < nHA * nc; e += 32) G[e] = 0.0;
       bool any = false;
       for (int j = 0; j < B.nprim; ++j) {
@@ -325,44 +322,46 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
         const double alpha = p * q * (rs * rs);
         const double X = Px - pb[1], Y = Py - pb[2], Z = Pz - pb[3];
         const double T = alpha * fma(X, X, fma(Y, Y, Z * Z));
-        __syncwarp();                                // the previous G step is done with Ek and R
-        if (lane < 3) gen_e1d(q, pb[5 + lane], pb[8 + lane], B.lP, B.lQ, Ek + lane * kGenE1);
+        __syncwarp();                                // the previous G step is done with R
         gen_seeds(L, alpha, rs, T, a.boys, base, lane);
         __syncwarp();
         const double* R = gen_rtab(L, X, Y, Z, base, R0, R1, lane);
-        const int ja = (int)pb[14], jb = (int)pb[15];
+        const EView Ej(a.coef, pb, B);
+        int h = lane / nc, cc = lane - (lane / nc) * nc;
         for (int e = lane; e < nHA * nc; e += 32) {
-          const int h = e / nc, cc = e - h * nc;
           const unsigned tv = g_tuv.v[h];
           const int t = tv & 255, u = (tv >> 8) & 255, v = tv >> 16;
-          const int cd = c0 + cc, ic = cd / nfJ, jd = cd - ic * nfJ;
-          const int fI = B.fP + ic, fJ = B.fQ + jd;
-          const int cx = a.lmn[3 * fI], cy = a.lmn[3 * fI + 1], cz = a.lmn[3 * fI + 2];
-          const int dx = a.lmn[3 * fJ], dy = a.lmn[3 * fJ + 1], dz = a.lmn[3 * fJ + 2];
-          const double s = ket_sum(Ek + (cx * 4 + dx) * 7, Ek + kGenE1 + (cy * 4 + dy) * 7,
-                                   Ek + 2 * kGenE1 + (cz * 4 + dz) * 7, cx + dx, cy + dy, cz + dz, t, u, v, R);
-          G[e] = fma(gcoef(a, fI, ja) * gcoef(a, fJ, jb) * kpb, s, G[e]);
+          const int cd = c0 + cc;
+          const unsigned d = __ldg(a.desc + B.doff + cd);
+          const int cx = dsc(d, 0), dx = dsc(d, 1), cy = dsc(d, 2), dy = dsc(d, 3), cz = dsc(d, 4), dz = dsc(d, 5);
+          const double s = ket_sum(Ej.ax(0, cx, dx), Ej.ax(1, cy, dy), Ej.ax(2, cz, dz), cx + dx, cy + dy, cz + dz,
+                                   t, u, v, R);
+          G[e] = fma(Ej.w(cd), s, G[e]);
+          h += dq;
+          cc += dr;
+          if (cc >= nc) { cc -= nc; ++h; }
         }
       }
       __syncwarp();
       if (!any) continue;
+      int ab = lane / nc, cc = lane - (lane / nc) * nc;
       for (int e = lane; e < nA * nc; e += 32) {
-        const int ab = e / nc, cc = e - ab * nc;
-        const int pp = ab / nfQ, qq = ab - pp * nfQ;
-        const int fP = A.fP + pp, fQ = A.fQ + qq;
-        const int ax = a.lmn[3 * fP], ay = a.lmn[3 * fP + 1], az = a.lmn[3 * fP + 2];
-        const int bx = a.lmn[3 * fQ], by = a.lmn[3 * fQ + 1], bz = a.lmn[3 * fQ + 2];
-        const double* ex = Eb + (ax * 4 + bx) * 7;
-        const double* ey = Eb + kGenE1 + (ay * 4 + by) * 7;
-        const double* ez = Eb + 2 * kGenE1 + (az * 4 + bz) * 7;
+        const unsigned d = __ldg(a.desc + A.doff + ab);
+        const int ax = dsc(d, 0), bx = dsc(d, 1), ay = dsc(d, 2), by = dsc(d, 3), az = dsc(d, 4), bz = dsc(d, 5);
+        const double* ex = Ei.ax(0, ax, bx);
+        const double* ey = Ei.ax(1, ay, by);
+        const double* ez = Ei.ax(2, az, bz);
         double s = 0.0;
         for (int t = 0; t <= ax + bx; ++t)
           for (int u = 0; u <= ay + by; ++u) {
             double sz = 0.0;
-            for (int v = 0; v <= az + bz; ++v) sz = fma(ez[v], G[gtet(t, u, v) * nc + cc], sz);
-            s = fma(ex[t] * ey[u], sz, s);
+            for (int v = 0; v <= az + bz; ++v) sz = fma(__ldg(ez + v), G[gtet(t, u, v) * nc + cc], sz);
+            s = fma(__ldg(ex + t) * __ldg(ey + u), sz, s);
           }
-        O[e] = fma(gcoef(a, fP, ia) * gcoef(a, fQ, ib) * kpa, s, O[e]);
+        O[e] = fma(Ei.w(ab), s, O[e]);
+        ab += dq;
+        cc += dr;
+        if (cc >= nc) { cc -= nc; ++ab; }
       }
     }
     __syncwarp();
@@ -427,49 +426,39 @@ __global__ void __launch_bounds__(32 * kGenWarps) k_gen_schwarz(const GenArgs a,
   double* base = gsm + warp * kGenWarpDoubles;
   double* R0 = base + 16;
   double* R1 = R0 + kGenR;
-  double* Eb = R1 + kGenR;
-  double* Ek = Eb + kGenE;
-  double* acc = Ek + kGenE;
+  double* acc = R1 + kGenR;
   const GenPairRec A = a.pairs[gidx[w]];
   const int nfQ = A.nfQ, nA = A.nfP * nfQ, L = 2 * (A.lP + A.lQ);
   for (int e = lane; e < nA; e += 32) acc[e] = 0.0;
   for (int i = 0; i < A.nprim; ++i) {
     const double* pi = a.prims + (size_t)(A.poff + i) * kGenPrimStride;
-    const double p = pi[0], kpi = pi[4];
-    const int ia = (int)pi[14], ib = (int)pi[15];
-    __syncwarp();
-    if (lane < 3) gen_e1d(p, pi[5 + lane], pi[8 + lane], A.lP, A.lQ, Eb + lane * kGenE1);
+    const double p = pi[0];
+    const EView Ei(a.coef, pi, A);
     for (int j = 0; j < A.nprim; ++j) {
       const double* pj = a.prims + (size_t)(A.poff + j) * kGenPrimStride;
-      const double q = pj[0], kpj = pj[4];
+      const double q = pj[0];
       const double pq = p + q, rs = rsqrt(pq), alpha = p * q * (rs * rs);
       const double X = pi[1] - pj[1], Y = pi[2] - pj[2], Z = pi[3] - pj[3];
       const double T = alpha * (X * X + Y * Y + Z * Z);
-      const int ja = (int)pj[14], jb = (int)pj[15];
+      const EView Ej(a.coef, pj, A);
       __syncwarp();
-      if (lane < 3) gen_e1d(q, pj[5 + lane], pj[8 + lane], A.lP, A.lQ, Ek + lane * kGenE1);
       gen_seeds(L, alpha, rs, T, a.boys, base, lane);
       __syncwarp();
       const double* R = gen_rtab(L, X, Y, Z, base, R0, R1, lane);
       for (int e = lane; e < nA; e += 32) {
-        const int pp = e / nfQ, qq = e - pp * nfQ;
-        const int fP = A.fP + pp, fQ = A.fQ + qq;
-        const int ax = a.lmn[3 * fP], ay = a.lmn[3 * fP + 1], az = a.lmn[3 * fP + 2];
-        const int bx = a.lmn[3 * fQ], by = a.lmn[3 * fQ + 1], bz = a.lmn[3 * fQ + 2];
+        const unsigned d = __ldg(a.desc + A.doff + e);
+        const int ax = dsc(d, 0), bx = dsc(d, 1), ay = dsc(d, 2), by = dsc(d, 3), az = dsc(d, 4), bz = dsc(d, 5);
         const int nx = ax + bx, ny = ay + by, nz = az + bz;
-        const double* kx = Ek + (ax * 4 + bx) * 7;
-        const double* ky = Ek + kGenE1 + (ay * 4 + by) * 7;
-        const double* kz = Ek + 2 * kGenE1 + (az * 4 + bz) * 7;
-        const double* ex = Eb + (ax * 4 + bx) * 7;
-        const double* ey = Eb + kGenE1 + (ay * 4 + by) * 7;
-        const double* ez = Eb + 2 * kGenE1 + (az * 4 + bz) * 7;
+        const double* ex = Ei.ax(0, ax, bx);
+        const double* ey = Ei.ax(1, ay, by);
+        const double* ez = Ei.ax(2, az, bz);
         double s = 0.0;
         for (int t = 0; t <= nx; ++t)
           for (int u = 0; u <= ny; ++u)
-            for (int v = 0; v <= nz; ++v) s = fma(ex[t] * ey[u] * ez[v], ket_sum(kx, ky, kz, nx, ny, nz, t, u, v, R), s);
-        const double wi = gcoef(a, fP, ia) * gcoef(a, fQ, ib) * kpi;
-        const double wj = gcoef(a, fP, ja) * gcoef(a, fQ, jb) * kpj;
-        acc[e] = fma(wi * wj, s, acc[e]);
+            for (int v = 0; v <= nz; ++v)
+              s = fma(__ldg(ex + t) * __ldg(ey + u) * __ldg(ez + v),
+                      ket_sum(Ej.ax(0, ax, bx), Ej.ax(1, ay, by), Ej.ax(2, az, bz), nx, ny, nz, t, u, v, R), s);
+        acc[e] = fma(Ei.w(e) * Ej.w(e), s, acc[e]);
       }
     }
   }
@@ -487,9 +476,8 @@ GenArgs make_args(const sqb::GenPath& g) {
   memset(&a, 0, sizeof(a));
   a.pairs = g.d_pairs;
   a.prims = g.d_prims;
-  a.lmn = g.d_lmn;
-  a.foff = g.d_foff;
-  a.ncoef = g.d_ncoef;
+  a.coef = g.d_coef;
+  a.desc = g.d_desc;
   a.boys = g.d_boys;
   a.counters = g.d_counters;
   return a;
@@ -514,9 +502,33 @@ int set_smem() {
 
 namespace sqb {
 
+// 1-D Hermite coefficients E^{ij}_t (i, j <= 3, t <= i+j) of a primitive pair along one axis:
+// E^{00}_0 = 1, E^{i+1,j}_t = E^{ij}_{t-1}/(2p) + X_PA E^{ij}_t + (t+1) E^{ij}_{t+1}, likewise in
+// j with X_PB.
+static void hermite_1d(double p, double xpa, double xpb, double E[4][4][7]) {
+  memset(E, 0, sizeof(double) * 4 * 4 * 7);
+  const double h = 0.5 / p;
+  E[0][0][0] = 1.0;
+  for (int i = 0; i <= 3; ++i)
+    for (int j = 0; j <= 3; ++j) {
+      if (i == 0 && j == 0) continue;
+      const bool up = i > 0;
+      const int si = up ? i - 1 : i, sj = up ? j : j - 1;
+      const double X = up ? xpa : xpb;
+      for (int t = 0; t <= i + j; ++t) {
+        double v = X * E[si][sj][t];
+        if (t > 0) v += h * E[si][sj][t - 1];
+        if (t + 1 <= si + sj) v += (t + 1) * E[si][sj][t + 1];
+        E[i][j][t] = v;
+      }
+    }
+}
+
 void gen_build_pairs(GenPath& g, const std::vector<GenShell>& sh, const double* schwarz, int nbf) {
   g.pairs.clear();
   g.prims.clear();
+  g.coef.clear();
+  g.desc.clear();
   g.gen_idx.clear();
   const int ns = (int)sh.size();
   struct Tmp { double s; int P, Q; };
@@ -539,8 +551,15 @@ void gen_build_pairs(GenPath& g, const std::vector<GenShell>& sh, const double* 
     rec.nprim = A.nprim * B.nprim;
     rec.poff = (int)(g.prims.size() / kGenPrimStride);
     rec.gen = (A.gen || B.gen) ? 1 : 0;
-    rec.pad_ = 0;
+    rec.doff = (int)g.desc.size();
     rec.schwarz = t.s;
+    for (int fa = 0; fa < A.nfunc; ++fa)
+      for (int fb = 0; fb < B.nfunc; ++fb) {
+        const int* la = A.lmn + 3 * fa;
+        const int* lb = B.lmn + 3 * fb;
+        g.desc.push_back(la[0] | lb[0] << 2 | la[1] << 4 | lb[1] << 6 | la[2] << 8 | lb[2] << 10);
+      }
+    const int lq1 = B.lmax + 1, lt = A.lmax + B.lmax + 1;
     // primitive data as the class kernels' pair records compute it (same expressions, so the
     // prefactor cut decides alike)
     const double ab2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
@@ -550,27 +569,34 @@ void gen_build_pairs(GenPath& g, const std::vector<GenShell>& sh, const double* 
         const double Px = (a * A.x + b * B.x) / p, Py = (a * A.y + b * B.y) / p, Pz = (a * A.z + b * B.z) / p;
         const double kp = std::exp(-a * b * ab2 / p) / p;
         const double f[kGenPrimStride] = {p, Px, Py, Pz, kp, Px - A.x, Py - A.y, Pz - A.z, Px - B.x, Py - B.y,
-                                          Pz - B.z, 0.0, 0.0, 0.0, (double)i, (double)j};
+                                          Pz - B.z, (double)g.coef.size(), 0.0, 0.0, (double)i, (double)j};
         g.prims.insert(g.prims.end(), f, f + kGenPrimStride);
+        // its 1-D Hermite tables, axis-major, [i][j][t] for i <= lP, j <= lQ; then the weights
+        const double PA3[3] = {Px - A.x, Py - A.y, Pz - A.z}, PB3[3] = {Px - B.x, Py - B.y, Pz - B.z};
+        for (int d = 0; d < 3; ++d) {
+          double E[4][4][7];
+          hermite_1d(p, PA3[d], PB3[d], E);
+          for (int ii = 0; ii <= A.lmax; ++ii)
+            for (int jj = 0; jj < lq1; ++jj)
+              for (int tt = 0; tt < lt; ++tt) g.coef.push_back(E[ii][jj][tt]);
+        }
+        for (int fa = 0; fa < A.nfunc; ++fa)
+          for (int fb = 0; fb < B.nfunc; ++fb) g.coef.push_back(A.coef[i * 16 + fa] * B.coef[j * 16 + fb] * kp);
       }
     if (rec.gen) g.gen_idx.push_back((int)g.pairs.size());
     g.pairs.push_back(rec);
   }
 }
 
-int gen_upload(GenPath& g, int nbf, const int* nprim, const int* lmn, const double* ncoefs, cudaStream_t st) {
-  std::vector<int> foff(nbf);
-  size_t tot = 0;
-  for (int i = 0; i < nbf; ++i) { foff[i] = (int)tot; tot += nprim[i]; }
+int gen_upload(GenPath& g, cudaStream_t st) {
   const std::vector<double> tab = boys_table(kGenBoysCols);
   struct Slot { void** dst; size_t bytes; const void* src; };
   const Slot slots[] = {
       {(void**)&g.d_pairs, g.pairs.size() * sizeof(GenPairRec), g.pairs.data()},
       {(void**)&g.d_prims, g.prims.size() * sizeof(double), g.prims.data()},
+      {(void**)&g.d_coef, g.coef.size() * sizeof(double), g.coef.data()},
+      {(void**)&g.d_desc, g.desc.size() * sizeof(int), g.desc.data()},
       {(void**)&g.d_gen_idx, g.gen_idx.size() * sizeof(int), g.gen_idx.data()},
-      {(void**)&g.d_lmn, (size_t)nbf * 3 * sizeof(int), lmn},
-      {(void**)&g.d_foff, (size_t)nbf * sizeof(int), foff.data()},
-      {(void**)&g.d_ncoef, tot * sizeof(double), ncoefs},
       {(void**)&g.d_boys, tab.size() * sizeof(double), tab.data()},
       {(void**)&g.d_counters, 2 * sizeof(unsigned long long), nullptr},
   };
@@ -660,10 +686,9 @@ void gen_free(GenPath& g) {
   g.bytes = 0;
   g.d_pairs = nullptr;
   g.d_prims = nullptr;
+  g.d_coef = nullptr;
+  g.d_desc = nullptr;
   g.d_gen_idx = nullptr;
-  g.d_lmn = nullptr;
-  g.d_foff = nullptr;
-  g.d_ncoef = nullptr;
   g.d_boys = nullptr;
   g.d_counters = nullptr;
 }

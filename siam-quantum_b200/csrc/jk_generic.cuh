@@ -19,6 +19,8 @@ struct GenShell {
   int gen;                          // 1: its pairs take the generic path
   double x, y, z;
   const double* exps;               // nprim exponents
+  const double* coef;               // norm * coefficient of primitive k, function f: coef[k * 16 + f]
+  const int* lmn;                   // l, m, n of function f: lmn[3 f .. 3 f + 2]
 };
 
 // One shell pair (P >= Q in the sorted shell order), 56 bytes.
@@ -26,12 +28,14 @@ struct GenPairRec {
   int P, Q, fP, fQ;
   int nfP, nfQ, lP, lQ;             // function counts and highest l+m+n of each shell
   int nprim, poff;                  // primitive pairs; first record (records of kGenPrimStride)
-  int gen, pad_;                    // gen: the pair has a generic shell
+  int gen;                          // the pair has a generic shell
+  int doff;                         // its function pairs' component descriptors in `desc`
   double schwarz;                   // max over the block of the basis-level Schwarz matrix
 };
 
 // Fields of one primitive-pair record: p, Px, Py, Pz, kp = exp(-ab|AB|^2/p)/p, PA (3), PB (3),
-// and the two primitive indices (as doubles), padded to 16.
+// the offset of its Hermite tables and weights in `coef` (as a double), padding, and the two
+// primitive indices (as doubles): 16.
 constexpr int kGenPrimStride = 16;
 
 // A CTA's unit: one generic bra pair and kets k0 .. k0+cnt-1 of the all-pairs list.  er: in
@@ -44,16 +48,17 @@ struct GenPath {
   bool on = false;                  // the basis has generic shells
   std::vector<GenPairRec> pairs;    // every shell pair, by decreasing Schwarz bound
   std::vector<double> prims;
+  std::vector<double> coef;         // per primitive pair: its 1-D Hermite tables, then its weights
+  std::vector<int> desc;            // per pair: one component descriptor per function pair
   std::vector<int> gen_idx;         // positions of the generic pairs in `pairs`
   // device (one allocation)
   void* d_base = nullptr;
   size_t bytes = 0;
   GenPairRec* d_pairs = nullptr;
   double* d_prims = nullptr;
+  double* d_coef = nullptr;
+  int* d_desc = nullptr;
   int* d_gen_idx = nullptr;
-  int* d_lmn = nullptr;             // per function l, m, n
-  int* d_foff = nullptr;            // per function: first primitive in d_ncoef
-  double* d_ncoef = nullptr;        // norm * coefficient per primitive
   double* d_boys = nullptr;         // Boys table, BOYS_NGRID x kGenBoysCols
   unsigned long long* d_counters = nullptr;   // quartets, primitive quartets of the last build
 };
@@ -75,8 +80,8 @@ struct GenBuild {
 
 // Pair records and primitive data for every shell pair; `schwarz` is the basis-level matrix.
 void gen_build_pairs(GenPath& g, const std::vector<GenShell>& sh, const double* schwarz, int nbf);
-// Device copies of the pair data, the basis arrays and the generic Boys table.
-int gen_upload(GenPath& g, int nbf, const int* nprim, const int* lmn, const double* ncoefs, cudaStream_t st);
+// Device copies of the pair data and the generic Boys table.
+int gen_upload(GenPath& g, cudaStream_t st);
 // Schwarz entries sqrt|(pq|pq)| of the generic pairs' functions into S (nbf x nbf, device).
 int gen_schwarz(const GenPath& g, int nbf, double* S, cudaStream_t st);
 // Work items of one build at these cutoffs; cost: a relative estimate for launch ordering.
