@@ -302,8 +302,10 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
       __syncwarp();
       continue;
     }
-    // lane steps through the (row, column) entries of an rows x nc block: 32 = dq*nc + dr
+    // lane steps through the entries of a block: 32 = dq*nc + dr (O, column fastest) and
+    // 32 = dc*nHA + dh (G, Hermite index fastest)
     const int dq = 32 / nc, dr = 32 - dq * nc;
+    const int dc = 32 / nHA, dh = 32 - dc * nHA;
     for (int e = lane; e < nA * nc; e += 32) O[e] = 0.0;
     for (int i = 0; i < A.nprim; ++i) {
       const double* pa = a.prims + (size_t)(A.poff + i) * kGenPrimStride;
@@ -327,7 +329,9 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
         __syncwarp();
         const double* R = gen_rtab(L, X, Y, Z, base, R0, R1, lane);
         const EView Ej(a.coef, pb, B);
-        int h = lane / nc, cc = lane - (lane / nc) * nc;
+        // Hermite index fastest across the lanes: neighbouring lanes share a ket function pair,
+        // so the loop bounds of ket_sum agree across them
+        int cc = lane / nHA, h = lane - (lane / nHA) * nHA;
         for (int e = lane; e < nHA * nc; e += 32) {
           const unsigned tv = g_tuv.v[h];
           const int t = tv & 255, u = (tv >> 8) & 255, v = tv >> 16;
@@ -336,10 +340,10 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
           const int cx = dsc(d, 0), dx = dsc(d, 1), cy = dsc(d, 2), dy = dsc(d, 3), cz = dsc(d, 4), dz = dsc(d, 5);
           const double s = ket_sum(Ej.ax(0, cx, dx), Ej.ax(1, cy, dy), Ej.ax(2, cz, dz), cx + dx, cy + dy, cz + dz,
                                    t, u, v, R);
-          G[e] = fma(Ej.w(cd), s, G[e]);
-          h += dq;
-          cc += dr;
-          if (cc >= nc) { cc -= nc; ++h; }
+          G[h * nc + cc] = fma(Ej.w(cd), s, G[h * nc + cc]);
+          h += dh;
+          cc += dc;
+          if (h >= nHA) { h -= nHA; ++cc; }
         }
       }
       __syncwarp();

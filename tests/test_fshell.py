@@ -240,3 +240,92 @@ def test_fshell_unsupported_entry_points_fail_loudly():
                                      out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), None)
     assert rc == -2 and b"f shells" in lib.sqb200_last_error()
     eng.close()
+
+
+def _perm_d_components(b):
+    """The basis with every d shell's six components in reverse order (a layout the class
+    kernels do not take: those shells go to the generic path), and the permutation p with
+    new function k = old function p[k]."""
+    sqb = load_sqb200()
+    n = b.nbf
+    perm = np.arange(n)
+    k = 0
+    while k < n:
+        if b.lmn[k].sum() == 2 and k + 5 < n and (b.lmn[k:k + 6].sum(axis=1) == 2).all():
+            perm[k:k + 6] = perm[k:k + 6][::-1]
+            k += 6
+        else:
+            k += 1
+    off = np.concatenate([[0], np.cumsum(b.nprim)])
+    ex = np.concatenate([b.exps[off[i]:off[i + 1]] for i in perm])
+    co = np.concatenate([b.coefs[off[i]:off[i + 1]] for i in perm])
+    nm = np.concatenate([b.norms[off[i]:off[i + 1]] for i in perm])
+    return sqb.basis.Basis(b.nprim[perm], b.lmn[perm], b.center[perm], ex, co, nm), perm
+
+
+@pytest.mark.gpu
+def test_reordered_d_components_take_the_generic_path():
+    """d shells whose components come in another order than the reference's run on the
+    generic path: J/K must equal the class kernels' result on the canonical order, permuted
+    (same screening: the block maxima do not change), and the oracle port's on the new order."""
+    sqb = load_sqb200()
+    g = golden("h2co_631gs")
+    b = golden_basis(g)
+    bp, perm = _perm_d_components(b)
+    assert (perm != np.arange(b.nbf)).any()
+    P = g["PA"]
+    Pp = P[np.ix_(perm, perm)]
+    e0 = sqb.JKEngine(b, schwarz=g["schwarz"])
+    J0, K0, _ = e0.build(P, restricted=True, scf_cutoff=1e-10)
+    q0 = e0.stats()["quartets"]
+    e0.close()
+    e1 = sqb.JKEngine(bp)                            # Schwarz bounds from the device, generic pairs included
+    np.testing.assert_allclose(e1.schwarz(), g["schwarz"][np.ix_(perm, perm)], rtol=1e-12, atol=1e-14)
+    J1, K1, _ = e1.build(Pp, restricted=True, scf_cutoff=1e-10)
+    assert e1.stats()["quartets"] == q0
+    e1.close()
+    assert np.abs(J1 - J0[np.ix_(perm, perm)]).max() <= TOL
+    assert np.abs(K1 - K0[np.ix_(perm, perm)]).max() <= TOL
+    Jp, Kp, _, _ = port.jk_build(bp, port.schwarz(bp), Pp, scf_cutoff=1e-10)
+    assert np.abs(J1 - Jp).max() <= TOL and np.abs(K1 - Kp).max() <= TOL
+
+
+@pytest.mark.gpu
+def test_merged_shell_takes_the_generic_path():
+    """An s and a d function with the same exponent on the same centre, adjacent in the basis,
+    form one seven-function shell (genGTOShell merges them; the reference types it TYPEX).
+    With screening off, its J/K equal those of the same functions placed apart (a separate s
+    and d shell, class kernels), up to the order of the functions."""
+    sqb = load_sqb200()
+    B = sqb.basis
+    atoms = sqb.molecules.to_bohr(sqb.molecules.water())
+    base = B.build_basis(atoms, "321g")
+    o = tuple(base.center[0])
+    extra_s = [(1, (0, 0, 0), o, 0.8)]
+    extra_d = [(1, lmn, o, 0.8) for lmn, _ in B.COMPONENTS["D"]]
+
+    def make(funcs):
+        nprim, lmn, cen, ex, co, nm = [], [], [], [], [], []
+        for np_, l, c, e, cf in funcs:
+            nprim.append(np_); lmn.append(l); cen.append(c)
+            ex.extend(e); co.extend(cf); nm.extend(B.prim_norm(x, *l) for x in e)
+        return B.Basis(nprim, lmn, cen, ex, co, nm)
+
+    off = np.concatenate([[0], np.cumsum(base.nprim)])
+    orig = [(int(base.nprim[i]), tuple(base.lmn[i]), tuple(base.center[i]), list(base.exps[off[i]:off[i + 1]]),
+             list(base.coefs[off[i]:off[i + 1]])) for i in range(base.nbf)]
+    new = [(1, l, c, [e], [1.0]) for _, l, c, e in extra_s + extra_d]
+    merged = make(orig + new)                        # ... s(0.8) d(0.8): one 7-function shell
+    apart = make(new[:1] + orig + new[1:])           # s(0.8) first, d(0.8) last: two shells
+    n = merged.nbf
+    perm = np.concatenate([np.arange(1, base.nbf + 1), [0], np.arange(base.nbf + 1, n)])   # apart index of merged k
+    rng = np.random.default_rng(2)
+    A = rng.normal(size=(n, n)); A = 0.2 * (A + A.T)
+    em, ea = sqb.JKEngine(merged), sqb.JKEngine(apart)
+    Jm, Km, _ = em.build(A, restricted=True, scf_cutoff=0.0, dscreen_rmax=float("inf"))
+    Pa = np.empty_like(A)
+    Pa[np.ix_(perm, perm)] = A
+    Ja, Ka, _ = ea.build(Pa, restricted=True, scf_cutoff=0.0, dscreen_rmax=float("inf"))
+    em.close(); ea.close()
+    assert np.abs(Jm - Ja[np.ix_(perm, perm)]).max() <= TOL
+    assert np.abs(Km - Ka[np.ix_(perm, perm)]).max() <= TOL
