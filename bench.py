@@ -6,7 +6,7 @@ the reference's GTO_JK_Matrix_Quartet_Parallel (src/matrix.c:3773) in its direct
 (Schwarz cutoff 1e-10, density-weighted screen on every quartet, no integral cache).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload c60|benzene|water|h2co|c60-synthetic|organics|serve]
+                  [--workload c60|benzene|water|h2co|water-qzp|c60-synthetic|organics|serve]
 
 Default workload: RHF/6-31G C60 (Ih, 6:6 bonds 1.40, 6:5 bonds 1.45 angstrom; 540 functions)
 from the reference's own converged SCF density (tests/golden/c60_631g.npz, made by running the
@@ -72,6 +72,11 @@ def workload(name, sqb):
         desc = {"benzene": "benzene RHF/6-31G* (D6h, 102 bf)", "water": "water RHF/3-21G (13 bf)",
                 "h2co": "formaldehyde RHF/6-31G* (34 bf)"}[name]
         return atoms, str(g["basis"]), np.array(g["PA"]), True, desc + ", converged density"
+    if name == "water-qzp":
+        g = np.load(os.path.join(ROOT, "tests", "golden", "water_qzp.npz"))
+        atoms = [(int(a[0]), a[1], a[2], a[3]) for a in g["atoms"]]
+        return (atoms, str(g["basis"]), np.array(g["PA"]), True,
+                "water RHF/QZP (126 bf; two f shells on O, one per H), converged density")
     if name == "c60":
         atoms, PA = c60_reference_density()
         return (atoms, "631g", PA, True,
@@ -585,7 +590,8 @@ def run_reference_split(args, atoms, bname, PA, desc, procs, sqb):
 # kernel, from one `ncu --set full` capture of the same workload; the summary with its command
 # is profiles/<kernel>_<workload>.md.  Kernels without a capture report null.
 TRAFFIC = {("benzene", "jk_DL_LL_R"): 912384, ("benzene", "jk_DL_LL_R_w"): 845312,
-           ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768, ("c60", "jk_LL_LL_R_w"): 20852224}
+           ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768, ("c60", "jk_LL_LL_R_w"): 20852224,
+           ("water-qzp", "k_jk_gen"): 1665536}
 
 
 def max_over_ranks(dist, t_local, device):
@@ -705,10 +711,11 @@ def run_ours(args, sqb):
     dom32 = dom["class"].endswith(" f32")
     total_flops = sum(r["flops"] for r in prof)
     peak = fp32_peak if dom32 else fp64_peak
+    # (the generic kernel of quartets with f shells counts the operations it executes)
+    dom_name = "k_jk_gen" if dom["class"].startswith("generic") else "jk_" + dom["class"].replace(" f32", "").replace("|", "_") + (
+        "_R_f32" if dom32 else {1: "_R_w", 2: "_R_s"}.get(int(tiles[dom["index"]]) if dom["index"] < len(tiles) else 0, "_R"))
     roof = {"bound": "fp32" if dom32 else "fp64",
-            "kernel": "jk_" + dom["class"].replace(" f32", "").replace("|", "_") + (
-                "_R_f32" if dom32 else {1: "_R_w", 2: "_R_s"}.get(
-                    int(tiles[dom["index"]]) if dom["index"] < len(tiles) else 0, "_R")),
+            "kernel": dom_name,
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "peak_source": "measured %s FMA peak of this GPU in this run (sqb200_peak_fma); "
                            "MEASURED_PEAKS.json has no FP64/FP32 figure" % ("FP32" if dom32 else "FP64"),
@@ -721,7 +728,7 @@ def run_ours(args, sqb):
         roof["traffic"] = tb
         roof["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/%s" % (
             {"benzene": "jk_DL_LL_R_forms_benzene_631gs.md", "c60-synthetic": "jk_LL_LL_R_w_c60_631g_synthetic.md",
-             "c60": "jk_LL_LL_R_w_c60_631g_refdensity.md"}.get(
+             "c60": "jk_LL_LL_R_w_c60_631g_refdensity.md", "water-qzp": "k_jk_gen_water_qzp.md"}.get(
                 args.workload, args.workload))
     line = {"metric": METRIC, "value": value, "unit": "builds/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
@@ -781,7 +788,7 @@ def main():
                     help="untimed steps (default 5 builds; 1 batch of solves for organics)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c60",
-                    choices=["c60", "benzene", "water", "h2co", "c60-synthetic", "organics", "serve"])
+                    choices=["c60", "benzene", "water", "h2co", "water-qzp", "c60-synthetic", "organics", "serve"])
     ap.add_argument("--nmol", type=int, default=256, help="molecules of the organics workload")
     ap.add_argument("--nreq", type=int, default=32, help="requests of the serve workload")
     ap.add_argument("--rates", default="0.5,1,2", help="mean arrival rates (1/s) of the serve workload")

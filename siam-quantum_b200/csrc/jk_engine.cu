@@ -1596,10 +1596,11 @@ int sqb200_jk_stats(sqb200_jk* c, long long* out, int n) {
     fl += (long long)kernel_flops(c, v, &h[4 * v]);
   }
   if (c->gen.on) {
-    unsigned long long g2[2];
+    unsigned long long g2[3];
     CUDA_OK(cudaMemcpy(g2, c->gen.d_counters, sizeof(g2), cudaMemcpyDeviceToHost));
     q += (long long)g2[0];
     pq += (long long)g2[1];
+    fl += (long long)g2[2];
   }
   long long v[6] = {q, pq, fl, (long long)c->ns, 0, (long long)c->last_launches};
   for (int k = 0; k < sqb::kNumPairClasses; ++k) v[4] += (long long)c->cls[k].pairs.size();
@@ -1645,7 +1646,7 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
   c->events.clear();
   std::vector<unsigned long long> h(8 * sqb::kNumClassKernels);
   CUDA_OK(cudaMemcpy(h.data(), c->d_counters, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
-  unsigned long long g2[2] = {0, 0};
+  unsigned long long g2[3] = {0, 0, 0};
   if (c->gen.on) CUDA_OK(cudaMemcpy(g2, c->gen.d_counters, sizeof(g2), cudaMemcpyDeviceToHost));
   int r = 0;
   for (int v = 0; v <= kGenericKernel && r < max_rows; ++v) {
@@ -1654,8 +1655,9 @@ int sqb200_jk_profile_read(sqb200_jk* c, double* rows, int max_rows, int* nrows)
     row[0] = v;
     row[1] = (double)c->prof_launches[v];
     row[2] = c->prof_ms[v];
-    // (the generic path reports no operation count)
-    row[3] = v == kGenericKernel ? 0.0 : kernel_flops(c, v, &h[4 * v]);
+    // (the generic path counts the operations it executes: Boys seeds, R recursion, the ket and
+    // bra Hermite sums and the digestion)
+    row[3] = v == kGenericKernel ? (double)g2[2] : kernel_flops(c, v, &h[4 * v]);
     row[4] = v == kGenericKernel ? (double)g2[1] : (double)h[4 * v + 1];
     row[5] = v == kGenericKernel ? (double)g2[0] : (double)h[4 * v];
     ++r;

@@ -278,7 +278,7 @@ __device__ double gen_mpole_err(const GenArgs& a, const GenPairRec& A, const Gen
 // substitutes the monopole values for the integrals (no primitive work), erx >= 0 records the
 // largest monopole error of the exact block in the bank's scratch.
 __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPairRec& B, double deg, double* W, int lane,
-                            unsigned long long& npq, bool mpq, int erx) {
+                            unsigned long long& npq, bool mpq, int erx, unsigned long long& nfl) {
   double* base = W;
   double* R0 = base + 16;
   double* R1 = R0 + kGenR;
@@ -328,6 +328,12 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
         gen_seeds(L, alpha, rs, T, a.boys, base, lane);
         __syncwarp();
         const double* R = gen_rtab(L, X, Y, Z, base, R0, R1, lane);
+        // operations of the Boys seeds (about 20 per order) and of the R recursion (3 per entry)
+        if (lane == 0) {
+          unsigned long long r = 20ull * (L + 1);
+          for (int top = 1; top <= L; ++top) r += 3ull * (top + 1) * (top + 2) * (top + 3) / 6;
+          nfl += r;
+        }
         const EView Ej(a.coef, pb, B);
         // Hermite index fastest across the lanes: neighbouring lanes share a ket function pair,
         // so the loop bounds of ket_sum agree across them
@@ -341,6 +347,7 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
           const double s = ket_sum(Ej.ax(0, cx, dx), Ej.ax(1, cy, dy), Ej.ax(2, cz, dz), cx + dx, cy + dy, cz + dz,
                                    t, u, v, R);
           G[h * nc + cc] = fma(Ej.w(cd), s, G[h * nc + cc]);
+          nfl += 2ull * ((cx + dx + 1) * (cy + dy + 1) * (cz + dz + 2) + 1);
           h += dh;
           cc += dc;
           if (h >= nHA) { h -= nHA; ++cc; }
@@ -363,6 +370,7 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
             s = fma(__ldg(ex + t) * __ldg(ey + u), sz, s);
           }
         O[e] = fma(Ei.w(ab), s, O[e]);
+        nfl += 2ull * ((ax + bx + 1) * (ay + by + 1) * (az + bz + 2) + 1);
         ab += dq;
         cc += dr;
         if (cc >= nc) { cc -= nc; ++ab; }
@@ -374,6 +382,8 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
       if (lane == 0) atomicMax(a.b.erscr + erx, (unsigned long long)__double_as_longlong(e) | (1ull << 63));
     }
     gen_digest(a, A, B, deg, O, c0, nc, lane);
+    // digestion: two J and four K products per integral and spin
+    if (lane == 0) nfl += 2ull * nA * nc * (2 + 4 * (a.b.uhf ? 2 : 1));
     __syncwarp();
   }
 }
@@ -384,7 +394,7 @@ __global__ void __launch_bounds__(32 * kGenWarps) k_jk_gen(const GenArgs a, cons
   double* W = gsm + warp * kGenWarpDoubles;
   const GenItem it = items[blockIdx.x];
   const GenPairRec A = a.pairs[it.bra];
-  unsigned long long nq = 0, npq = 0;
+  unsigned long long nq = 0, npq = 0, nfl = 0;
   for (int kk = warp; kk < it.cnt; kk += kGenWarps) {
     const int kb = it.k0 + kk;
     const GenPairRec B = a.pairs[kb];
@@ -410,11 +420,17 @@ __global__ void __launch_bounds__(32 * kGenWarps) k_jk_gen(const GenArgs a, cons
     if (!ok) continue;
     const double deg = (A.P == A.Q ? 0.5 : 1.0) * (B.P == B.Q ? 0.5 : 1.0) * (kb == it.bra ? 0.5 : 1.0);
     ++nq;
-    gen_quartet(a, A, B, deg, W, lane, npq, mpq, erexp == sqb::ERR_UNKNOWN ? erx : -1);
+    gen_quartet(a, A, B, deg, W, lane, npq, mpq, erexp == sqb::ERR_UNKNOWN ? erx : -1, nfl);
   }
   if (lane == 0) {
     if (nq) atomicAdd(a.counters, nq);
     if (npq) atomicAdd(a.counters + 1, npq);
+  }
+  // operations: every lane counted its own share
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nfl += __shfl_xor_sync(0xffffffffu, nfl, o);
+  if (lane == 0) {
+    if (nfl) atomicAdd(a.counters + 2, nfl);
   }
 }
 
@@ -602,7 +618,7 @@ int gen_upload(GenPath& g, cudaStream_t st) {
       {(void**)&g.d_desc, g.desc.size() * sizeof(int), g.desc.data()},
       {(void**)&g.d_gen_idx, g.gen_idx.size() * sizeof(int), g.gen_idx.data()},
       {(void**)&g.d_boys, tab.size() * sizeof(double), tab.data()},
-      {(void**)&g.d_counters, 2 * sizeof(unsigned long long), nullptr},
+      {(void**)&g.d_counters, 3 * sizeof(unsigned long long), nullptr},
   };
   auto rnd = [](size_t b) { return (std::max<size_t>(b, 1) + 255) / 256 * 256; };
   size_t bytes = 0;
@@ -671,7 +687,7 @@ void gen_items(const GenPath& g, double outer, double fixed, std::vector<GenItem
 }
 
 int gen_launch(const GenPath& g, const GenItem* d_items, int nitems, const GenBuild& b, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(g.d_counters, 0, 2 * sizeof(unsigned long long), st);
+  cudaError_t e = cudaMemsetAsync(g.d_counters, 0, 3 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return set_error(SQB200_ECUDA, std::string("generic counters: ") + cudaGetErrorString(e));
   if (nitems <= 0) return SQB200_OK;
   int rc = set_smem();

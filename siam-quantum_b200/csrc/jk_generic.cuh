@@ -60,7 +60,7 @@ struct GenPath {
   int* d_desc = nullptr;
   int* d_gen_idx = nullptr;
   double* d_boys = nullptr;         // Boys table, BOYS_NGRID x kGenBoysCols
-  unsigned long long* d_counters = nullptr;   // quartets, primitive quartets of the last build
+  unsigned long long* d_counters = nullptr;   // quartets, primitive quartets, operations of the last build
 };
 
 // Arguments of one generic J/K launch (the accumulators are the build's unsymmetrised ones).
