@@ -73,6 +73,7 @@ SWAP_SMEM_O = int(os.environ.get("SQB_SWAP_SMEM", "0"))
 G_MAX_SWAP = int(os.environ.get("SQB_G_MAX_SWAP", "40"))   # G doubles per pass of that form
 G_MAX = int(os.environ.get("SQB_G_MAX", "48"))
 PREFETCH = int(os.environ.get("SQB_PREFETCH", "0"))      # software-pipeline the ket primitive loop
+TILE_KETS = int(os.environ.get("SQB_TILE_KETS", "1"))    # passes over (c, d) tiles of the ket functions
 # the wide form stages the ket primitive fields a pass reads in shared memory, one record ahead
 # (cp.async double buffer, thread-private slots), instead of reading them from global memory
 STAGE_WIDE = int(os.environ.get("SQB_STAGE_WIDE", "0"))
@@ -203,6 +204,31 @@ def ket_per_pass(bra, ket, state_max, smem_o=False):
     return min(per, len(fk))
 
 
+def ket_blocks(ncd, nc, nd, per):
+    """The ket function pairs cd = c*nd + d of each pass.  Every pass digests into K rows of the
+    bra functions at the columns of its distinct c and its distinct d, one atomic per (bra
+    function, column) and pass, so a pass covering a tc x td tile of (c, d) adds (tc + td) x
+    (bra functions) instead of (1 + per) for a run of one c: tiles when they need no more passes
+    than runs of consecutive pairs (TILE_KETS=0 keeps the runs)."""
+    runs = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
+    if not TILE_KETS or nc < 2 or nd < 2 or per < 2:
+        return runs
+    best = None
+    for tc in range(1, nc + 1):
+        for td in range(1, nd + 1):
+            if tc * td > per:
+                continue
+            npass = -(-nc // tc) * -(-nd // td)
+            key = (npass, tc + td)
+            if best is None or key < best[0]:
+                best = (key, tc, td)
+    (npass, _), tc, td = best
+    if npass > len(runs):
+        return runs
+    return [[c * nd + d for c in range(c0, min(nc, c0 + tc)) for d in range(d0, min(nd, d0 + td))]
+            for c0 in range(0, nc, tc) for d0 in range(0, nd, td)]
+
+
 def n_passes(bra, ket, state_max, smem_o=False):
     fk, _, _ = etable(ket)
     per = ket_per_pass(bra, ket, state_max, smem_o)
@@ -229,7 +255,7 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
     NB = 5 + len(layb)
     NK = 5 + len(layk)
     per = ket_per_pass(bra, ket, (STATE_MAX_F32 if F32 else STATE_MAX) if state_max is None else state_max, smem_o)
-    blocks = [list(range(s, min(ncd, s + per))) for s in range(0, ncd, per)]
+    blocks = ket_blocks(ncd, len(COMP[ket[0]]), len(COMP[ket[1]]), per)
     name = "jk_%s_%s_%s%s%s" % (bra, ket, spin, "_f32" if F32 else "", suffix)
     SO = smem_o and not F32
     ST = stage and not F32 and not SO and not PREFETCH
