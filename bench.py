@@ -12,8 +12,9 @@ Default workload: RHF/6-31G C60 (Ih, 6:6 bonds 1.40, 6:5 bonds 1.45 angstrom; 54
 from the reference's own converged SCF density (tests/golden/c60_631g.npz, made by running the
 reference), Schwarz 1e-10 and the density screen on every quartet, as the reference's direct
 mode builds it.  benzene = RHF/6-31G* benzene (D6h, C-C 1.39, C-H 1.09 angstrom; 102
-functions) from its converged density; c60-synthetic = C60 with a seeded synthetic density and
-the density screen off.  Multi-GPU runs are independent replicas (one molecule's build runs on
+functions) from its converged density; water-qzp = RHF/QZP water (126 functions, f shells on
+every atom: the generic quartet kernel) from its converged density; c60-synthetic = C60 with a
+seeded synthetic density and the density screen off.  Multi-GPU runs are independent replicas (one molecule's build runs on
 one GPU and is not sharded), value = all ranks' builds / max-over-ranks time.
 
 The reference arm (--impl reference) and the cpu_baseline of C60 run the reference's own process
