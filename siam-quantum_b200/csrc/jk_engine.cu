@@ -2595,11 +2595,11 @@ __device__ __forceinline__ double draise(double two_alpha, int i, double up, dou
   return two_alpha * up - (i > 0 ? i * down : 0.0);
 }
 
-__device__ __noinline__ void grad_quartet(int pq, int ij, const int2* __restrict__ pairs,
-                                          const GShell* __restrict__ shells, const double* __restrict__ exps,
-                                          const double* __restrict__ wts, const double* __restrict__ PT,
-                                          const double* __restrict__ PS, int nbf, const double* __restrict__ tab,
-                                          double* sg);
+__device__ __noinline__ void grad_quartet(int pq, int ij, int ka, int kb, const double* __restrict__ sEb,
+                                          const int2* __restrict__ pairs, const GShell* __restrict__ shells,
+                                          const double* __restrict__ exps, const double* __restrict__ wts,
+                                          const double* __restrict__ PT, const double* __restrict__ PS, int nbf,
+                                          const double* __restrict__ tab, double* gq);
 
 // Two-electron part of the gradient: one block per (bra pair, 128 ket pairs), one thread per
 // unique shell quartet (ket pair index <= bra pair index).
@@ -2611,14 +2611,43 @@ __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const dou
   // the block's contributions are summed per atom in shared memory first, then added to grad
   // with one atomic per touched component (grad has only 3 natom entries: atomics of every
   // thread straight into it collide)
+  // The bra pair is the block's: the 1-D Hermite tables of its current primitive pair (with one
+  // order more for the derivative) are built once per block in shared memory, by three threads
+  // (one per axis), and read by every thread (the same entries across a warp: broadcasts).
   extern __shared__ double sgrad[];
+  double* sEb = sgrad + 3 * natom;                 // [3][4][4][8]
   const int pq = blockIdx.y;
   if (pq >= npairs || (int)(blockIdx.x * blockDim.x) > pq) return;      // whole block: no quartet
   for (int x = threadIdx.x; x < 3 * natom; x += blockDim.x) sgrad[x] = 0.0;
-  __syncthreads();
   const int ij = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = ij <= pq && !(psch[pq] * psch[ij] * ppm[pq] * ppm[ij] < 1e-10);
-  if (live) grad_quartet(pq, ij, pairs, shells, exps, wts, PT, PS, nbf, tab, sgrad);
+  const int2 PQ = pairs[pq];
+  const GShell A = shells[PQ.x], B = shells[PQ.y];
+  double gq[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};      // d/dA, d/dB, d/dC (x, y, z each)
+  const bool any = __syncthreads_or(live);
+  for (int ka = 0; any && ka < A.nprim; ++ka)
+    for (int kb = 0; kb < B.nprim; ++kb) {
+      __syncthreads();                             // the previous primitive pair's readers are done
+      if (threadIdx.x < 3) {
+        const int d = threadIdx.x;
+        const double ea = exps[A.poff + ka], eb = exps[B.poff + kb], p = ea + eb;
+        const double Ad = d == 0 ? A.x : d == 1 ? A.y : A.z, Bd = d == 0 ? B.x : d == 1 ? B.y : B.z;
+        const double Pd = (ea * Ad + eb * Bd) / p;
+        herm1d<4, 4, 8>(p, Pd - Ad, Pd - Bd, A.lmax + 1, B.lmax + 1, reinterpret_cast<double (*)[4][8]>(sEb + 128 * d));
+      }
+      __syncthreads();
+      if (live) grad_quartet(pq, ij, ka, kb, sEb, pairs, shells, exps, wts, PT, PS, nbf, tab, gq);
+    }
+  if (live) {
+    const int2 IJ = pairs[ij];
+    const int ac = shells[IJ.x].atom, ad = shells[IJ.y].atom;
+    for (int x = 0; x < 3; ++x) {
+      atomicAdd(sgrad + 3 * A.atom + x, gq[x]);
+      atomicAdd(sgrad + 3 * B.atom + x, gq[3 + x]);
+      atomicAdd(sgrad + 3 * ac + x, gq[6 + x]);
+      atomicAdd(sgrad + 3 * ad + x, -(gq[x] + gq[3 + x] + gq[6 + x]));
+    }
+  }
   if (__syncthreads_or(live))
     for (int x = threadIdx.x; x < 3 * natom; x += blockDim.x) {
       const double v = sgrad[x];
@@ -2626,30 +2655,27 @@ __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const dou
     }
 }
 
-// One shell quartet (pairs[pq] | pairs[ij]) of k_grad_eri, its contributions added to sg
-// (3 per atom, shared memory).
-__device__ __noinline__ void grad_quartet(int pq, int ij, const int2* __restrict__ pairs,
-                                          const GShell* __restrict__ shells, const double* __restrict__ exps,
-                                          const double* __restrict__ wts, const double* __restrict__ PT,
-                                          const double* __restrict__ PS, int nbf, const double* __restrict__ tab,
-                                          double* sg) {
+// Bra primitive pair (ka, kb) of one shell quartet (pairs[pq] | pairs[ij]) of k_grad_eri, its
+// contributions added to gq (d/dA, d/dB, d/dC); sEb holds the bra pair's Hermite tables.
+__device__ __noinline__ void grad_quartet(int pq, int ij, int ka, int kb, const double* __restrict__ sEb,
+                                          const int2* __restrict__ pairs, const GShell* __restrict__ shells,
+                                          const double* __restrict__ exps, const double* __restrict__ wts,
+                                          const double* __restrict__ PT, const double* __restrict__ PS, int nbf,
+                                          const double* __restrict__ tab, double* gq) {
   const int2 PQ = pairs[pq], IJ = pairs[ij];
   const GShell A = shells[PQ.x], B = shells[PQ.y], C = shells[IJ.x], D = shells[IJ.y];
   const double deg = (PQ.x == PQ.y ? 0.5 : 1.0) * (IJ.x == IJ.y ? 0.5 : 1.0) * (pq == ij ? 0.5 : 1.0);
   const int Lb = A.lmax + B.lmax + 1, L = A.lmax + B.lmax + C.lmax + D.lmax + 1;
   double g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-  double Eb[3][4][4][8], Ek[3][4][4][8];
+  const double (*Eb)[4][4][8] = reinterpret_cast<const double (*)[4][4][8]>(sEb);
+  double Ek[3][4][4][8];
   double F[GR_MAXL + 1], R[GR_NT], tmp[GR_NT], V[4][56];
   const double ab2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
   const double cd2 = (C.x - D.x) * (C.x - D.x) + (C.y - D.y) * (C.y - D.y) + (C.z - D.z) * (C.z - D.z);
-  for (int ka = 0; ka < A.nprim; ++ka)
-    for (int kb = 0; kb < B.nprim; ++kb) {
+  {
       const double ea = exps[A.poff + ka], eb = exps[B.poff + kb], p = ea + eb;
       const double Px = (ea * A.x + eb * B.x) / p, Py = (ea * A.y + eb * B.y) / p, Pz = (ea * A.z + eb * B.z) / p;
       const double Kab = exp(-ea * eb / p * ab2);
-      herm1d<4, 4, 8>(p, Px - A.x, Px - B.x, A.lmax + 1, B.lmax + 1, Eb[0]);
-      herm1d<4, 4, 8>(p, Py - A.y, Py - B.y, A.lmax + 1, B.lmax + 1, Eb[1]);
-      herm1d<4, 4, 8>(p, Pz - A.z, Pz - B.z, A.lmax + 1, B.lmax + 1, Eb[2]);
       for (int kc = 0; kc < C.nprim; ++kc)
         for (int kd = 0; kd < D.nprim; ++kd) {
           const double ec = exps[C.poff + kc], ed = exps[D.poff + kd], q = ec + ed;
@@ -2762,10 +2788,9 @@ __device__ __noinline__ void grad_quartet(int pq, int ij, const int2* __restrict
         }
     }
   for (int x = 0; x < 3; ++x) {
-    atomicAdd(sg + 3 * A.atom + x, g[0][x]);
-    atomicAdd(sg + 3 * B.atom + x, g[1][x]);
-    atomicAdd(sg + 3 * C.atom + x, g[2][x]);
-    atomicAdd(sg + 3 * D.atom + x, -(g[0][x] + g[1][x] + g[2][x]));
+    gq[x] += g[0][x];
+    gq[3 + x] += g[1][x];
+    gq[6 + x] += g[2][x];
   }
 }
 
@@ -2954,8 +2979,8 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   }
   const int npairs = (int)pairs.size();
   if (npairs > 65535) return fail(SQB200_EINVAL, "sqb200_gradient: more than 65535 shell pairs");
-  if (3 * (size_t)natom * sizeof(double) > 48 * 1024)   // per-block atom sums of k_grad_eri
-    return fail(SQB200_EINVAL, "sqb200_gradient: more than 2048 atoms");
+  if ((3 * (size_t)natom + 3 * 128) * sizeof(double) > 48 * 1024)   // k_grad_eri: atom sums + bra tables
+    return fail(SQB200_EINVAL, "sqb200_gradient: more than 1920 atoms");
   std::vector<double> PT(nn), PS(nn);
   for (size_t i = 0; i < nn; ++i) { PT[i] = PA[i] + PB[i]; PS[i] = PA[i] - PB[i]; }
   void* d[16] = {nullptr};
@@ -2985,7 +3010,7 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, 3 * natom * sizeof(double), c->stream);
   if (e == cudaSuccess) {
     if (terms & SQB200_GRAD_ERI)
-      k_grad_eri<<<dim3((npairs + 127) / 128, npairs), 128, 3 * natom * sizeof(double), c->stream>>>(
+      k_grad_eri<<<dim3((npairs + 127) / 128, npairs), 128, (3 * natom + 3 * 128) * sizeof(double), c->stream>>>(
           npairs, (const int2*)dp, (const double*)dsch, (const double*)dpm, (const GShell*)d[12], (const double*)d[13],
           (const double*)d[14], (const double*)d[9], (const double*)d[10], n, c->d_boys, natom, (double*)dg);
     if (terms & (SQB200_GRAD_HCORE | SQB200_GRAD_OVERLAP))

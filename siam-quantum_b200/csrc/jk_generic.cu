@@ -365,8 +365,18 @@ __device__ void gen_quartet(const GenArgs& a, const GenPairRec& A, const GenPair
         double s = 0.0;
         for (int t = 0; t <= ax + bx; ++t)
           for (int u = 0; u <= ay + by; ++u) {
+            // G row gtet(t, u, v) for v = 0, 1, ...: n = t+u+v and m = u+v rise together
+            int n = t + u, m = u;
+            int row = n * (n + 1) * (n + 2) / 6 + m * (m + 1) / 2;
+            int dn = (n + 1) * (n + 2) / 2;
             double sz = 0.0;
-            for (int v = 0; v <= az + bz; ++v) sz = fma(__ldg(ez + v), G[gtet(t, u, v) * nc + cc], sz);
+            for (int v = 0; v <= az + bz; ++v) {
+              sz = fma(__ldg(ez + v), G[row * nc + cc], sz);
+              row += dn + m + 2;
+              dn += n + 2;
+              ++n;
+              ++m;
+            }
             s = fma(__ldg(ex + t) * __ldg(ey + u), sz, s);
           }
         O[e] = fma(Ei.w(ab), s, O[e]);
