@@ -243,8 +243,11 @@ int sqb200_segdots_destroy(sqb200_segdots *plan);
  * GradEri_ShellSet_Parallel (src/grad.c:1734) -- as uhf_force (src/grad.c:2155) assembles
  * them.  PA, PB: the densities of the final orbitals; W: the energy-weighted density
  * sum_i e_i C_i C_i^T over the occupied orbitals of both spins (host arrays, nbf*nbf).  Every
- * basis function must sit on one of the nuclei.  Limits: at most 65535 shell pairs and 2048
- * atoms (SQB200_EINVAL beyond).  Synchronous. */
+ * basis function must sit on one of the nuclei.  Functions up to f in shells of at most 10
+ * functions (SQB200_EUNSUPPORTED beyond); at most 65535 shell pairs and about 1800 atoms
+ * (SQB200_EINVAL beyond).  The two-electron screens are the reference's (1e-10 on shell
+ * quartets and on function quartets of a primitive quartet); the environment variable
+ * SQB200_GRAD_SCREEN replaces that threshold (0 keeps every quartet).  Synchronous. */
 int sqb200_gradient(sqb200_jk *ctx, int natom, const double *Z, const double *axyz,
                     const double *PA, const double *PB, const double *W, double *grad);
 

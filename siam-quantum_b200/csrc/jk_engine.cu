@@ -2504,31 +2504,47 @@ extern "C" int sqb200_syev_batched(int device, int n, int batch, double* A, doub
 // (the reference's 0.5 PT PT - 0.25 (PT PT + PS PS) summed over the eight index permutations),
 // shell quartets skipped when Sch(PQ) Sch(IJ) maxPT(PQ) maxPT(IJ) < 1e-10, primitive quartets
 // below the 1e-15 prefactor cut, and, as the reference does, a function quartet of a primitive
-// quartet whose density factor times prefactor and weights is below 1e-10.  Derivatives of a primitive by its centre raise and lower
+// quartet whose density factor times prefactor and weights is below 1e-10 (both 1e-10 screens
+// follow SQB200_GRAD_SCREEN when it is set).  Derivatives of a primitive by its centre raise and lower
 // its angular momentum, d/dA_x g_a = 2 alpha g_{a+1x} - a_x g_{a-1x}; the fourth centre follows
 // from translational invariance.  The integrals are McMurchie-Davidson with runtime loops (one
 // thread per shell quartet or function pair): a correctness-first form, not tuned.
 
 namespace {
 
+constexpr int GR_NF = 10;   // functions of one shell the gradient kernels take (an f shell)
+
 struct GShell {
   int first, nfunc, nprim, poff;   // poff: first primitive in the exps / wts arrays
   int lmax, atom;
   double x, y, z;
-  int lmn[6][3];
+  int lmn[GR_NF][3];
 };
 
-#define GR_MAXL 9                  // highest Hermite order: (dd|dd) + 1
-#define GR_NT 220                  // tetra(GR_MAXL) entries
+// Array bounds of the gradient kernels for functions up to l = LG (2: d, 3: f): the highest
+// Hermite order of a quartet with one index raised ((dd|dd) + 1 = 9, (ff|ff) + 1 = 13), its
+// tetrahedral R table, the 1-D Hermite tables E^{ij}_t with i, j <= LG + 1 (the raised index)
+// and t <= 2 LG + 2 (the one-electron tables raise j by two more for the kinetic term), and the
+// bra-side intermediates V (t+u+v <= 2 LG + 1).
+template <int LG>
+struct GDim {
+  static constexpr int MAXL = 4 * LG + 1;
+  static constexpr int NT = (MAXL + 1) * (MAXL + 2) * (MAXL + 3) / 6;
+  static constexpr int NI = LG + 2;
+  static constexpr int NJ1 = LG + 3;
+  static constexpr int NTT = 2 * LG + 4;
+  static constexpr int NV = (2 * LG + 2) * (2 * LG + 3) * (2 * LG + 4) / 6;
+  static constexpr int NE = 3 * NI * NI * NTT;   // doubles of one pair's three tables
+};
 
-// F_0..F_M (M <= 9, runtime) from the same grid as boys<M>: the top order by the Taylor
+// F_0..F_M (M <= 13, runtime) from a Boys table of ncol columns: the top order by the Taylor
 // expansion with as many terms as the table's columns allow, then downward recursion.
-__device__ void boys_rt(int M, double T, const double* __restrict__ tab, double* F) {
+__device__ void boys_rt(int M, double T, const double* __restrict__ tab, int ncol, double* F) {
   if (T < BOYS_TMAX) {
     const int g = __double2int_rn(T * BOYS_INV_H);
     const double d = T - g * BOYS_H;
-    const double* row = tab + g * BOYS_NCOL + M;
-    const int nt = min(BOYS_NTAY, BOYS_NCOL - M);
+    const double* row = tab + g * ncol + M;
+    const int nt = min(BOYS_NTAY, ncol - M);
     double s = row[nt - 1];
     for (int k = nt - 2; k >= 0; --k) s = fma(s, -d * (1.0 / (double)(k + 1)), row[k]);
     F[M] = s;
@@ -2567,8 +2583,9 @@ __device__ void herm1d(double p, double xpa, double xpb, int imax, int jmax, dou
 }
 
 // R_tuv (order 0) for t+u+v <= L into R (tetra index), from base[n] = (-2 a)^n F_n
+template <int LG>
 __device__ void herm_R(int L, double a, double X, double Y, double Z, const double* F, double* R, double* tmp) {
-  double base[GR_MAXL + 1];
+  double base[GDim<LG>::MAXL + 1];
   double w = 1.0;
   for (int n = 0; n <= L; ++n) { base[n] = w * F[n]; w *= -2.0 * a; }
   double* cur = (L % 2 == 0) ? R : tmp;
@@ -2595,19 +2612,23 @@ __device__ __forceinline__ double draise(double two_alpha, int i, double up, dou
   return two_alpha * up - (i > 0 ? i * down : 0.0);
 }
 
+template <int LG>
 __device__ __noinline__ void grad_quartet(int pq, int ij, int ka, int kb, const double* __restrict__ sEb,
                                           const int2* __restrict__ pairs, const GShell* __restrict__ shells,
                                           const double* __restrict__ exps, const double* __restrict__ wts,
                                           const double* __restrict__ PT, const double* __restrict__ PS, int nbf,
-                                          const double* __restrict__ tab, double* gq);
+                                          const double* __restrict__ tab, int ncol, double screen, double* gq);
 
 // Two-electron part of the gradient: one block per (bra pair, 128 ket pairs), one thread per
 // unique shell quartet (ket pair index <= bra pair index).
+template <int LG>
 __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const double* __restrict__ psch,
                            const double* __restrict__ ppm, const GShell* __restrict__ shells,
                            const double* __restrict__ exps, const double* __restrict__ wts,
                            const double* __restrict__ PT, const double* __restrict__ PS, int nbf,
-                           const double* __restrict__ tab, int natom, double* __restrict__ grad) {
+                           const double* __restrict__ tab, int ncol, double screen, int natom,
+                           double* __restrict__ grad) {
+  using GD = GDim<LG>;
   // the block's contributions are summed per atom in shared memory first, then added to grad
   // with one atomic per touched component (grad has only 3 natom entries: atomics of every
   // thread straight into it collide)
@@ -2615,12 +2636,12 @@ __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const dou
   // order more for the derivative) are built once per block in shared memory, by three threads
   // (one per axis), and read by every thread (the same entries across a warp: broadcasts).
   extern __shared__ double sgrad[];
-  double* sEb = sgrad + 3 * natom;                 // [3][4][4][8]
+  double* sEb = sgrad + 3 * natom;                 // [3][NI][NI][NTT]
   const int pq = blockIdx.y;
   if (pq >= npairs || (int)(blockIdx.x * blockDim.x) > pq) return;      // whole block: no quartet
   for (int x = threadIdx.x; x < 3 * natom; x += blockDim.x) sgrad[x] = 0.0;
   const int ij = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = ij <= pq && !(psch[pq] * psch[ij] * ppm[pq] * ppm[ij] < 1e-10);
+  const bool live = ij <= pq && !(psch[pq] * psch[ij] * ppm[pq] * ppm[ij] < screen);
   const int2 PQ = pairs[pq];
   const GShell A = shells[PQ.x], B = shells[PQ.y];
   double gq[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};      // d/dA, d/dB, d/dC (x, y, z each)
@@ -2633,10 +2654,11 @@ __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const dou
         const double ea = exps[A.poff + ka], eb = exps[B.poff + kb], p = ea + eb;
         const double Ad = d == 0 ? A.x : d == 1 ? A.y : A.z, Bd = d == 0 ? B.x : d == 1 ? B.y : B.z;
         const double Pd = (ea * Ad + eb * Bd) / p;
-        herm1d<4, 4, 8>(p, Pd - Ad, Pd - Bd, A.lmax + 1, B.lmax + 1, reinterpret_cast<double (*)[4][8]>(sEb + 128 * d));
+        herm1d<GD::NI, GD::NI, GD::NTT>(p, Pd - Ad, Pd - Bd, A.lmax + 1, B.lmax + 1,
+                                     reinterpret_cast<double (*)[GD::NI][GD::NTT]>(sEb + GD::NE / 3 * d));
       }
       __syncthreads();
-      if (live) grad_quartet(pq, ij, ka, kb, sEb, pairs, shells, exps, wts, PT, PS, nbf, tab, gq);
+      if (live) grad_quartet<LG>(pq, ij, ka, kb, sEb, pairs, shells, exps, wts, PT, PS, nbf, tab, ncol, screen, gq);
     }
   if (live) {
     const int2 IJ = pairs[ij];
@@ -2657,19 +2679,21 @@ __global__ void k_grad_eri(int npairs, const int2* __restrict__ pairs, const dou
 
 // Bra primitive pair (ka, kb) of one shell quartet (pairs[pq] | pairs[ij]) of k_grad_eri, its
 // contributions added to gq (d/dA, d/dB, d/dC); sEb holds the bra pair's Hermite tables.
+template <int LG>
 __device__ __noinline__ void grad_quartet(int pq, int ij, int ka, int kb, const double* __restrict__ sEb,
                                           const int2* __restrict__ pairs, const GShell* __restrict__ shells,
                                           const double* __restrict__ exps, const double* __restrict__ wts,
                                           const double* __restrict__ PT, const double* __restrict__ PS, int nbf,
-                                          const double* __restrict__ tab, double* gq) {
+                                          const double* __restrict__ tab, int ncol, double screen, double* gq) {
+  using GD = GDim<LG>;
   const int2 PQ = pairs[pq], IJ = pairs[ij];
   const GShell A = shells[PQ.x], B = shells[PQ.y], C = shells[IJ.x], D = shells[IJ.y];
   const double deg = (PQ.x == PQ.y ? 0.5 : 1.0) * (IJ.x == IJ.y ? 0.5 : 1.0) * (pq == ij ? 0.5 : 1.0);
   const int Lb = A.lmax + B.lmax + 1, L = A.lmax + B.lmax + C.lmax + D.lmax + 1;
   double g[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-  const double (*Eb)[4][4][8] = reinterpret_cast<const double (*)[4][4][8]>(sEb);
-  double Ek[3][4][4][8];
-  double F[GR_MAXL + 1], R[GR_NT], tmp[GR_NT], V[4][56];
+  const double (*Eb)[GD::NI][GD::NI][GD::NTT] = reinterpret_cast<const double (*)[GD::NI][GD::NI][GD::NTT]>(sEb);
+  double Ek[3][GD::NI][GD::NI][GD::NTT];
+  double F[GD::MAXL + 1], R[GD::NT], tmp[GD::NT], V[4][GD::NV];
   const double ab2 = (A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z);
   const double cd2 = (C.x - D.x) * (C.x - D.x) + (C.y - D.y) * (C.y - D.y) + (C.z - D.z) * (C.z - D.z);
   {
@@ -2683,18 +2707,18 @@ __device__ __noinline__ void grad_quartet(int pq, int ij, int ka, int kb, const 
           const double pre = TWO_PI_2_5 * Kab * Kcd / (p * q * sqrt(p + q));
           if (pre < PRIM_CUTOFF) continue;
           const double Qx = (ec * C.x + ed * D.x) / q, Qy = (ec * C.y + ed * D.y) / q, Qz = (ec * C.z + ed * D.z) / q;
-          herm1d<4, 4, 8>(q, Qx - C.x, Qx - D.x, C.lmax + 1, D.lmax, Ek[0]);
-          herm1d<4, 4, 8>(q, Qy - C.y, Qy - D.y, C.lmax + 1, D.lmax, Ek[1]);
-          herm1d<4, 4, 8>(q, Qz - C.z, Qz - D.z, C.lmax + 1, D.lmax, Ek[2]);
+          herm1d<GD::NI, GD::NI, GD::NTT>(q, Qx - C.x, Qx - D.x, C.lmax + 1, D.lmax, Ek[0]);
+          herm1d<GD::NI, GD::NI, GD::NTT>(q, Qy - C.y, Qy - D.y, C.lmax + 1, D.lmax, Ek[1]);
+          herm1d<GD::NI, GD::NI, GD::NTT>(q, Qz - C.z, Qz - D.z, C.lmax + 1, D.lmax, Ek[2]);
           const double al = p * q / (p + q);
           const double X = Px - Qx, Y = Py - Qy, Z = Pz - Qz;
-          boys_rt(L, al * (X * X + Y * Y + Z * Z), tab, F);
-          herm_R(L, al, X, Y, Z, F, R, tmp);
+          boys_rt(L, al * (X * X + Y * Y + Z * Z), tab, ncol, F);
+          herm_R<LG>(L, al, X, Y, Z, F, R, tmp);
           for (int c = 0; c < C.nfunc; ++c)
             for (int d = 0; d < D.nfunc; ++d) {
               const int* lc = C.lmn[c];
               const int* ld = D.lmn[d];
-              const double wcd = wts[(C.poff + kc) * 6 + c] * wts[(D.poff + kd) * 6 + d];
+              const double wcd = wts[(C.poff + kc) * GR_NF + c] * wts[(D.poff + kd) * GR_NF + d];
               if (wcd == 0.0) continue;
               // V0 = sum_k (-1)^k E^cd_k R_{h+k}; V1..3 the same with d/dC_{x,y,z} E^cd
               for (int N = 0; N <= Lb; ++N)
@@ -2733,13 +2757,13 @@ __device__ __noinline__ void grad_quartet(int pq, int ij, int ka, int kb, const 
                   const double gam = 4.0 * PT[fa * nbf + fb] * PT[fc * nbf + fd] -
                                      (PT[fa * nbf + fc] * PT[fb * nbf + fd] + PT[fa * nbf + fd] * PT[fb * nbf + fc] +
                                       PS[fa * nbf + fc] * PS[fb * nbf + fd] + PS[fa * nbf + fd] * PS[fb * nbf + fc]);
-                  const double wab = wts[(A.poff + ka) * 6 + a] * wts[(B.poff + kb) * 6 + b];
+                  const double wab = wts[(A.poff + ka) * GR_NF + a] * wts[(B.poff + kb) * GR_NF + b];
                   // the reference's per-primitive screen of one function quartet
                   // (src/grad.c:1982-1988): |coef r| < 1e-10, coef its density factor with the
                   // function-level degeneracy, r the primitive prefactor times the four weights
                   const double dfn = (fa == fb ? 0.5 : 1.0) * (fc == fd ? 0.5 : 1.0) *
                                      ((fa == fc && fb == fd) || (fa == fd && fb == fc) ? 0.5 : 1.0);
-                  if (fabs(gam * dfn * pre * wab * wcd) < 1e-10) continue;
+                  if (fabs(gam * dfn * pre * wab * wcd) < screen) continue;
                   const double G = deg * pre * wcd * wab * gam;
                   if (G == 0.0) continue;
                   const int* la = A.lmn[a];
@@ -2801,13 +2825,15 @@ namespace {
 // One-electron part of the gradient, one thread per ordered function pair (a, b):
 // -W_ab dS_ab, PT_ab d(T_ab + V_ab) on the atoms of a and b, and the Hellmann-Feynman term
 // PT_ab dV^C_ab / dC = -PT_ab (dV^C/dA + dV^C/dB) on every nucleus C.
+template <int LG>
 __global__ void k_grad_1e(int nbf, const int* __restrict__ nprim, const int* __restrict__ off,
                           const int* __restrict__ lmn, const double* __restrict__ xyz,
                           const double* __restrict__ exps, const double* __restrict__ nc,
                           const int* __restrict__ fatom, int natom, const double* __restrict__ Z,
-                          const double* __restrict__ axyz, const double* __restrict__ tab,
+                          const double* __restrict__ axyz, const double* __restrict__ tab, int ncol,
                           const double* __restrict__ PT, const double* __restrict__ W, double* __restrict__ grad,
                           int terms) {
+  using GD = GDim<LG>;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= nbf * nbf) return;
   const int ia = idx / nbf, ib = idx % nbf;
@@ -2818,8 +2844,8 @@ __global__ void k_grad_1e(int nbf, const int* __restrict__ nprim, const int* __r
   const int* lb = lmn + 3 * ib;
   const double* A = xyz + 3 * ia;
   const double* B = xyz + 3 * ib;
-  double E[3][4][5][8];
-  double F[GR_MAXL + 1], R[GR_NT], tmp[GR_NT];
+  double E[3][GD::NI][GD::NJ1][GD::NTT];
+  double F[GD::MAXL + 1], R[GD::NT], tmp[GD::NT];
   double gA[3] = {0, 0, 0};      // d/dA of PT (T + V) - W S (the B side is added by translational invariance)
   double gB[3] = {0, 0, 0};      // d/dB of PT V (kinetic and overlap: -d/dA)
   const double ab2 = (A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]);
@@ -2829,7 +2855,7 @@ __global__ void k_grad_1e(int nbf, const int* __restrict__ nprim, const int* __r
       const double a = exps[off[ia] + i], b = exps[off[ib] + j], p = a + b;
       const double c = nc[off[ia] + i] * nc[off[ib] + j] * exp(-a * b * ab2 / p);
       const double P[3] = {(a * A[0] + b * B[0]) / p, (a * A[1] + b * B[1]) / p, (a * A[2] + b * B[2]) / p};
-      for (int d = 0; d < 3; ++d) herm1d<4, 5, 8>(p, P[d] - A[d], P[d] - B[d], la[d] + 1, lb[d] + 2, E[d]);
+      for (int d = 0; d < 3; ++d) herm1d<GD::NI, GD::NJ1, GD::NTT>(p, P[d] - A[d], P[d] - B[d], la[d] + 1, lb[d] + 2, E[d]);
       const double sq = sqrt(M_PI / p);
       // 1-D overlap S(i,j) and kinetic T(i,j) factors and their d/dA
       double S0[3], T0[3], dS[3], dT[3];
@@ -2857,8 +2883,8 @@ __global__ void k_grad_1e(int nbf, const int* __restrict__ nprim, const int* __r
       // nuclear attraction: V^C = -Z_C (2 pi / p) sum_tuv E^ab_tuv R_tuv(p, P - C)
       for (int at = 0; at < natom; ++at) {
         const double X = P[0] - axyz[3 * at], Y = P[1] - axyz[3 * at + 1], Zc = P[2] - axyz[3 * at + 2];
-        boys_rt(L, p * (X * X + Y * Y + Zc * Zc), tab, F);
-        herm_R(L, p, X, Y, Zc, F, R, tmp);
+        boys_rt(L, p * (X * X + Y * Y + Zc * Zc), tab, ncol, F);
+        herm_R<LG>(L, p, X, Y, Zc, F, R, tmp);
         const double f = -Z[at] * (2.0 * M_PI / p) * c * pt;
         double vA[3] = {0, 0, 0}, vB[3] = {0, 0, 0};
         for (int t = 0; t <= la[0] + lb[0] + 1; ++t)
@@ -2924,20 +2950,23 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   const int ns = (int)c->shells.size();
   std::vector<GShell> gs(ns);
   std::vector<double> sex, swt;
+  int lmax_all = 0;
   for (int s = 0; s < ns; ++s) {
     const Shell& sh = c->shells[s];
     GShell& g = gs[s];
     g.first = sh.first; g.nfunc = sh.nfunc; g.nprim = sh.nprim; g.poff = (int)sex.size();
     g.lmax = 0;
+    if (sh.nfunc > GR_NF)
+      return fail(SQB200_EUNSUPPORTED, "sqb200_gradient: a shell of more than " + std::to_string(GR_NF) + " functions");
     for (int f = 0; f < sh.nfunc; ++f) {
       for (int d = 0; d < 3; ++d) g.lmn[f][d] = sh.lmn[f][d];
       g.lmax = std::max(g.lmax, sh.lmn[f][0] + sh.lmn[f][1] + sh.lmn[f][2]);
     }
-    if (g.lmax > 2) return fail(SQB200_EUNSUPPORTED, "sqb200_gradient: shells beyond d");
+    lmax_all = std::max(lmax_all, g.lmax);
     g.atom = fat[sh.first]; g.x = sh.x; g.y = sh.y; g.z = sh.z;
     for (int k = 0; k < sh.nprim; ++k) {
       sex.push_back(sh.exps[k]);
-      for (int f = 0; f < 6; ++f) swt.push_back(f < sh.nfunc ? sh.coef[k][f] : 0.0);
+      for (int f = 0; f < GR_NF; ++f) swt.push_back(f < sh.nfunc ? sh.coef[k][f] : 0.0);
     }
   }
   // shell pairs P >= Q with their Schwarz and |PT| block maxima
@@ -2979,8 +3008,20 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   }
   const int npairs = (int)pairs.size();
   if (npairs > 65535) return fail(SQB200_EINVAL, "sqb200_gradient: more than 65535 shell pairs");
-  if ((3 * (size_t)natom + 3 * 128) * sizeof(double) > 48 * 1024)   // k_grad_eri: atom sums + bra tables
-    return fail(SQB200_EINVAL, "sqb200_gradient: more than 1920 atoms");
+  // kernels sized for d (LG = 2) or f (LG = 3) functions; the f forms read the generic path's
+  // Boys table, whose 22 columns give orders to 13 their full Taylor expansion
+  if (lmax_all > 3) return fail(SQB200_EUNSUPPORTED, "sqb200_gradient: functions above f");
+  const bool fgrad = lmax_all > 2;
+  if (fgrad && !c->gen.d_boys) return fail(SQB200_EINVAL, "sqb200_gradient: no Boys table for f functions");
+  const double* btab = fgrad ? c->gen.d_boys : c->d_boys;
+  const int bcol = fgrad ? sqb::kGenBoysCols : BOYS_NCOL;
+  const size_t smem_eri = (3 * (size_t)natom + (fgrad ? GDim<3>::NE : GDim<2>::NE)) * sizeof(double);
+  // the two-electron screens (shell quartet, function quartet of a primitive quartet): the
+  // reference's 1e-10 unless SQB200_GRAD_SCREEN sets another (0 keeps every quartet)
+  double screen = 1e-10;
+  if (const char* ev = getenv("SQB200_GRAD_SCREEN")) screen = atof(ev);
+  if (smem_eri > 48 * 1024)   // k_grad_eri: atom sums + the bra pair's tables
+    return fail(SQB200_EINVAL, "sqb200_gradient: too many atoms (" + std::to_string(natom) + ") for the per-block sums");
   std::vector<double> PT(nn), PS(nn);
   for (size_t i = 0; i < nn; ++i) { PT[i] = PA[i] + PB[i]; PS[i] = PA[i] - PB[i]; }
   void* d[16] = {nullptr};
@@ -3009,14 +3050,25 @@ extern "C" int sqb200_gradient_terms(sqb200_jk* c, int natom, const double* Z, c
   cudaError_t e = up.upload(&base, c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dg, 0, 3 * natom * sizeof(double), c->stream);
   if (e == cudaSuccess) {
-    if (terms & SQB200_GRAD_ERI)
-      k_grad_eri<<<dim3((npairs + 127) / 128, npairs), 128, (3 * natom + 3 * 128) * sizeof(double), c->stream>>>(
+    const dim3 geri((npairs + 127) / 128, npairs);
+    if ((terms & SQB200_GRAD_ERI) && fgrad)
+      k_grad_eri<3><<<geri, 128, smem_eri, c->stream>>>(
           npairs, (const int2*)dp, (const double*)dsch, (const double*)dpm, (const GShell*)d[12], (const double*)d[13],
-          (const double*)d[14], (const double*)d[9], (const double*)d[10], n, c->d_boys, natom, (double*)dg);
-    if (terms & (SQB200_GRAD_HCORE | SQB200_GRAD_OVERLAP))
-      k_grad_1e<<<(int)((nn + 127) / 128), 128, 0, c->stream>>>(
+          (const double*)d[14], (const double*)d[9], (const double*)d[10], n, btab, bcol, screen, natom, (double*)dg);
+    else if (terms & SQB200_GRAD_ERI)
+      k_grad_eri<2><<<geri, 128, smem_eri, c->stream>>>(
+          npairs, (const int2*)dp, (const double*)dsch, (const double*)dpm, (const GShell*)d[12], (const double*)d[13],
+          (const double*)d[14], (const double*)d[9], (const double*)d[10], n, btab, bcol, screen, natom, (double*)dg);
+    const int g1 = (int)((nn + 127) / 128);
+    if ((terms & (SQB200_GRAD_HCORE | SQB200_GRAD_OVERLAP)) && fgrad)
+      k_grad_1e<3><<<g1, 128, 0, c->stream>>>(
           n, (const int*)d[0], (const int*)d[1], (const int*)d[2], (const double*)d[3], (const double*)d[4],
-          (const double*)d[5], (const int*)d[6], natom, (const double*)d[7], (const double*)d[8], c->d_boys,
+          (const double*)d[5], (const int*)d[6], natom, (const double*)d[7], (const double*)d[8], btab, bcol,
+          (const double*)d[9], (const double*)d[11], (double*)dg, terms);
+    else if (terms & (SQB200_GRAD_HCORE | SQB200_GRAD_OVERLAP))
+      k_grad_1e<2><<<g1, 128, 0, c->stream>>>(
+          n, (const int*)d[0], (const int*)d[1], (const int*)d[2], (const double*)d[3], (const double*)d[4],
+          (const double*)d[5], (const int*)d[6], natom, (const double*)d[7], (const double*)d[8], btab, bcol,
           (const double*)d[9], (const double*)d[11], (double*)dg, terms);
     e = cudaGetLastError();
   }

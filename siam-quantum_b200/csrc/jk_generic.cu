@@ -40,7 +40,7 @@ using sqb::GenItem;
 using sqb::GenPairRec;
 using sqb::kGenPrimStride;
 
-constexpr int kGenBoysCols = 22;                       // orders 0..21: F_12 + 8 Taylor terms
+using sqb::kGenBoysCols;
 constexpr int kGenR = 455;                             // tetrahedral entries with t+u+v <= 12
 constexpr int kGenWarps = 2;                           // warps per CTA
 constexpr int kGenKets = 16;                           // kets per work item

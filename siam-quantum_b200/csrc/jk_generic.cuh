@@ -12,6 +12,8 @@ namespace sqb {
 
 constexpr int kGenLmax = 3;         // highest l+m+n of one function on the generic path
 constexpr int kGenMmax = 4 * kGenLmax;   // highest Boys order, (ff|ff)
+constexpr int kGenBoysCols = 22;    // Boys table columns of the generic path: orders to 12 (13 for
+                                    // the f gradient) with their 9-term Taylor expansions
 
 // One shell as the generic path sees it.
 struct GenShell {

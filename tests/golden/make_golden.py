@@ -16,6 +16,8 @@ Usage:  make -C oracle && python tests/golden/make_golden.py
         python tests/golden/make_golden.py --iters    (add the reference's SCF iteration count)
         python tests/golden/make_golden.py --forces   (add the reference's forces, uhf_force)
         python tests/golden/make_golden.py --fshells  (the f-shell cases, FSHELL_CASES)
+        python tests/golden/make_golden.py --forces --fshells   (their forces)
+        python tests/golden/make_golden.py --fd       (finite-difference gradients of the f cases)
 """
 import os
 import subprocess
@@ -124,9 +126,9 @@ def add_scf_iters():
         print(name, "reference SCF iterations", res["iters"])
 
 
-def add_forces():
+def add_forces(cases=CASES):
     """Store the reference's forces (uhf_force after uhf(), 1STEP, SCFConv 1e-8)."""
-    for name, geom, bas, opts in CASES:
+    for name, geom, bas, opts in cases:
         path = os.path.join(OUT, name + ".npz")
         rec = dict(np.load(path, allow_pickle=True))
         with tempfile.TemporaryDirectory() as d:
@@ -138,6 +140,42 @@ def add_forces():
         rec["force"] = F
         np.savez_compressed(path, **rec)
         print(name, "reference forces", F.tolist())
+
+
+def add_fd_gradients(cases=FSHELL_CASES, h=2.5e-4):
+    """Store central finite differences of the reference's own SCF energy (uhf(), 1STEP,
+    SCFConv 1e-11) with respect to every nuclear coordinate, step h angstrom, as fd_grad
+    (hartree/bohr).  With f functions the reference's analytic forces (uhf_force) depart from
+    these, so the device gradient of the f cases is checked against them."""
+    from concurrent.futures import ThreadPoolExecutor
+    bohr = 0.52917721092
+
+    def energy(atoms, bas, opts):
+        with tempfile.TemporaryDirectory() as d:
+            xyz = os.path.join(d, "m.xyz")
+            with open(xyz, "w") as f:
+                f.write(M.xyz_text(atoms, "fd"))
+            res, _, _ = port.ref_scf(xyz, os.path.join(BASIS_DIR, bas + ".txt"),
+                                     ["-SCFACC=1STEP", "-SCFCONV=1e-11"] + list(opts))
+        return float(res["energy"])
+
+    for name, geom, bas, opts in cases:
+        atoms = geom()
+        jobs = []
+        for a in range(len(atoms)):
+            for x in range(3):
+                for sgn in (1, -1):
+                    at = [list(t) for t in atoms]
+                    at[a][1 + x] += sgn * h
+                    jobs.append([tuple(t) for t in at])
+        with ThreadPoolExecutor(max_workers=8) as ex:
+            E = list(ex.map(lambda at: energy(at, bas, opts), jobs))
+        fd = np.array([(E[2 * k] - E[2 * k + 1]) / (2 * h / bohr) for k in range(3 * len(atoms))]).reshape(-1, 3)
+        path = os.path.join(OUT, name + ".npz")
+        rec = dict(np.load(path, allow_pickle=True))
+        rec["fd_grad"] = fd
+        np.savez_compressed(path, **rec)
+        print(name, "finite-difference gradient", fd.tolist())
 
 
 def main(cases=CASES):
@@ -171,8 +209,10 @@ if __name__ == "__main__":
         add_oneint()
     elif "--iters" in sys.argv[1:]:
         add_scf_iters()
+    elif "--fd" in sys.argv[1:]:
+        add_fd_gradients()
     elif "--forces" in sys.argv[1:]:
-        add_forces()
+        add_forces(FSHELL_CASES if "--fshells" in sys.argv[1:] else CASES)
     elif "--fshells" in sys.argv[1:]:
         main(FSHELL_CASES)
     else:

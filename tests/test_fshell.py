@@ -140,6 +140,36 @@ def test_fshell_device_scf_energy(case):
     assert abs(iters - int(g["scf_iters"])) <= 1
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", FCASES)
+def test_fshell_gradient_against_finite_differences(case, monkeypatch):
+    """Nuclear gradient with f functions (the gradient kernels sized for f: raised indices to g,
+    Hermite orders to 13).  The reference's own uhf_force does not pin it: with f shells its
+    forces depart from finite differences of its own energy (water/QZP: 8.6e-5 hartree/bohr on
+    the oxygen's z, and 2.4e-4 normal to the molecular plane, where the gradient vanishes by
+    symmetry; its d-shell forces agree with the same finite differences to 1.4e-6).  So the
+    check is the central finite-difference gradient of the reference's SCF energy (fd_grad,
+    tests/golden/make_golden.py --fd): with every quartet kept (SQB200_GRAD_SCREEN=0) to 1e-6
+    hartree/bohr, with the reference's 1e-10 screens to 5e-5, and zero where symmetry makes it
+    zero."""
+    sqb = load_sqb200()
+    g = golden(case)
+    job = sqb.scf.SCFJob(_atoms(g), str(g["basis"]), restricted=bool(g["restricted"]))
+    job.run()
+    G0 = job.gradient()                                 # the reference's screens
+    monkeypatch.setenv("SQB200_GRAD_SCREEN", "0")
+    G = job.gradient()                                  # every quartet
+    job.close()
+    fd = g["fd_grad"]
+    assert np.abs(G.sum(axis=0)).max() < 1e-8           # translational invariance
+    assert np.abs(G - fd).max() <= 1e-6, np.abs(G - fd).max()
+    assert np.abs(G0 - fd).max() <= 5e-5, np.abs(G0 - fd).max()
+    xyz = np.array([a[1:] for a in _atoms(g)])
+    for ax in range(3):                                 # an axis no atom leaves: zero force along it
+        if np.abs(xyz[:, ax]).max() == 0.0:
+            assert np.abs(G[:, ax]).max() <= 1e-9 and np.abs(G0[:, ax]).max() <= 1e-9
+
+
 def _inputs(d, g):
     """The molecule and the basis text (written by the package) for a run of the reference."""
     sqb = load_sqb200()
