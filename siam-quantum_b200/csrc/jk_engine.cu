@@ -871,7 +871,8 @@ int ensure_side_streams(sqb200_jk* c) {
 // operations, the launch-order and stream-balancing estimate.
 void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra_base, int ket_base, int mol,
                  std::vector<sqb::WorkItem>& items, std::vector<sqb::WorkItem>& items32, double& cost64,
-                 double& cost32, std::vector<int>* ers = nullptr, long long* er_run = nullptr) {
+                 double& cost32, std::vector<int>* ers = nullptr, long long* er_run = nullptr,
+                 bool allow_f32 = true) {
   const sqb::ClassKernel& K = sqb::kClassKernels[ki];
   const PairClass& B = c->cls[K.bra_cls];
   const PairClass& T = c->cls[K.ket_cls];
@@ -882,7 +883,7 @@ void class_items(const sqb200_jk* c, int ki, double outer, double fixed, int bra
   // item records the error-bank slot of its first ket; the slots of each (bra, ket sub-list)
   // run are the outer-cutoff survivors in order, so the layout does not depend on `fixed`
   const bool mpm = er_run != nullptr;
-  const bool mixed = !mpm && c->fp32_below > 0.0 && K.fn_r32 != nullptr;
+  const bool mixed = allow_f32 && !mpm && c->fp32_below > 0.0 && K.fn_r32 != nullptr;
   // every (bra sub-list, ket sub-list) combination; inside one class each unordered pair of
   // sub-lists once, and inside one sub-list each unordered pair of pairs once (k >= b)
   for (size_t sx = 0; sx + 1 < B.sub.size(); ++sx)
@@ -964,6 +965,25 @@ void sort_heavy_first(std::vector<sqb::WorkItem>& v, size_t first, F nprims) {
   std::copy(tmp.begin(), tmp.end(), v.begin() + first);
 }
 
+// A class whose FP32 work items would number fewer than this runs all its quartets in FP64: a
+// second launch of a few hundred CTAs costs more than its FP32 arithmetic saves, and splitting
+// the ket ranges at the FP32 threshold leaves the FP64 items shorter (SQB200_F32_MIN_ITEMS,
+// default 600; measured on B200: benzene/6-31G* at tau 1e-5 0.896 ms with no minimum, 0.758
+// with 600, 0.744 with 1200, against 0.748 in FP64; C60 51.05 ms either way).
+size_t f32_min_items() {
+  static const size_t n = [] {
+    const char* e = getenv("SQB200_F32_MIN_ITEMS");
+    return e ? (size_t)std::max(0L, atol(e)) : (size_t)600;
+  }();
+  return n;
+}
+
+// True when a class's FP32 items are too few to launch: the class then runs all its quartets
+// in FP64, with the work items of a build without the FP32 split.
+bool too_few_f32(const std::vector<sqb::WorkItem>& items32) {
+  return !items32.empty() && items32.size() < f32_min_items();
+}
+
 int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) {
   const int mpm = c->mp_on ? 1 : 0;
   auto key = std::make_tuple(outer, fixed, mpm ? 0.0 : c->fp32_below, mpm);
@@ -982,6 +1002,12 @@ int build_work(sqb200_jk* c, double outer, double fixed, sqb200_jk::Work** out) 
     double cost64 = 0.0, cost32 = 0.0;
     class_items(c, ki, outer, fixed, 0, 0, 0, items, items32, cost64, cost32, mpm ? &ers : nullptr,
                 mpm ? &er_run : nullptr);
+    if (too_few_f32(items32)) {
+      items.resize(first);
+      items32.clear();
+      cost64 = cost32 = 0.0;
+      class_items(c, ki, outer, fixed, 0, 0, 0, items, items32, cost64, cost32, nullptr, nullptr, false);
+    }
     if (!mpm) {   // (multipole mode keeps the items with their bank slots in generation order)
       const PairClass& B = c->cls[sqb::kClassKernels[ki].bra_cls];
       const PairClass& T = c->cls[sqb::kClassKernels[ki].ket_cls];
@@ -2251,6 +2277,18 @@ extern "C" int sqb200_batch_set_step(sqb200_batch* b, const int* restricted, con
                     b->cls[K.ket_cls].pair_base[m], m, items, items32, c64, c32);
         sort_heavy_first(items, a64, np);
         sort_heavy_first(items32, a32, np);
+      }
+      if (too_few_f32(items32)) {
+        items.resize(f64);
+        items32.clear();
+        c64 = c32 = 0.0;
+        for (int m = 0; m < b->nmol; ++m) {
+          if (b->rec[m].uhf != sp) continue;
+          const size_t a64 = items.size();
+          class_items(b->mols[m], ki, scf_cutoff[m], fixed_cutoff[m], b->cls[K.bra_cls].pair_base[m],
+                      b->cls[K.ket_cls].pair_base[m], m, items, items32, c64, c32, nullptr, nullptr, false);
+          sort_heavy_first(items, a64, np);
+        }
       }
       if ((int)items.size() > f64) {
         b->kernel.push_back(ki); b->spin.push_back(sp); b->first.push_back(f64);
