@@ -135,6 +135,22 @@ def ref_jk(xyz_path, basis_path, PA, PB=None, restricted=True, cutoff=1e-10, max
     return m[0], m[1], m[2], res
 
 
+def ref_nosymm(xyz_path, basis_path, PA, PB=None, cutoff=0.0):
+    """The reference's unscreened quadruple loop over basis functions (GTO_JK_Matrix_NoSymm,
+    src/matrix.c:5098-5183, contracted integrals by contr_eri): GA = J[PA+PB] - K[PA] and GB
+    likewise with PB.  At cutoff 0 no quartet and no primitive is skipped."""
+    n = PA.shape[0]
+    with tempfile.TemporaryDirectory() as d:
+        pa = os.path.join(d, "pa.bin"); np.ascontiguousarray(PA, dtype=np.float64).tofile(pa)
+        pb = "-"
+        if PB is not None:
+            pb = os.path.join(d, "pb.bin"); np.ascontiguousarray(PB, dtype=np.float64).tofile(pb)
+        out = os.path.join(d, "out.bin")
+        ref_run(["nosymm", xyz_path, basis_path, pa, pb, "%.17g" % cutoff, out])
+        m = np.fromfile(out, dtype=np.float64).reshape(2, n, n)
+    return m[0], m[1]
+
+
 def ref_jkseq(xyz_path, basis_path, densities, cutoffs, scf_cutoff=1e-10, max_mem=250):
     """Visits of one reference SCF (sqref jkseq): after a reset, one restricted
     GTO_JK_Matrix_Quartet_Parallel per (density, fixedCutoff), its cached state carried from

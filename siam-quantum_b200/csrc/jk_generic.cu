@@ -51,6 +51,7 @@ constexpr size_t kGenSmem = (size_t)kGenWarps * kGenWarpDoubles * sizeof(double)
 static_assert(sqb::kGenMmax == 12 && (sqb::kGenMmax + 1) * (sqb::kGenMmax + 2) * (sqb::kGenMmax + 3) / 6 == kGenR,
               "R table size");
 static_assert(sizeof(GenPairRec) == 56, "pair record layout");
+static_assert(kGenSmem <= 48 * 1024, "the generic kernels launch without a shared-memory opt-in");
 
 // (t, u, v) of tetrahedral index k: order n = t+u+v, then m = u+v, then v ascending
 struct TuvTable {
@@ -513,21 +514,6 @@ GenArgs make_args(const sqb::GenPath& g) {
   return a;
 }
 
-int set_smem() {
-  static int done = 0;
-  static cudaError_t err = cudaSuccess;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (!(done & (1 << (dev & 31)))) {
-    err = cudaFuncSetAttribute(k_jk_gen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmem);
-    if (err == cudaSuccess)
-      err = cudaFuncSetAttribute(k_gen_schwarz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGenSmem);
-    if (err != cudaSuccess) return sqb::set_error(SQB200_ECUDA, std::string("generic kernels: ") + cudaGetErrorString(err));
-    done |= 1 << (dev & 31);
-  }
-  return SQB200_OK;
-}
-
 }  // namespace
 
 namespace sqb {
@@ -657,8 +643,6 @@ int gen_upload(GenPath& g, cudaStream_t st) {
 
 int gen_schwarz(const GenPath& g, int nbf, double* S, cudaStream_t st) {
   if (g.gen_idx.empty()) return SQB200_OK;
-  int rc = set_smem();
-  if (rc) return rc;
   const int ngen = (int)g.gen_idx.size();
   k_gen_schwarz<<<(ngen + kGenWarps - 1) / kGenWarps, 32 * kGenWarps, kGenSmem, st>>>(make_args(g), g.d_gen_idx, ngen,
                                                                                      nbf, S);
@@ -700,8 +684,6 @@ int gen_launch(const GenPath& g, const GenItem* d_items, int nitems, const GenBu
   cudaError_t e = cudaMemsetAsync(g.d_counters, 0, 3 * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return set_error(SQB200_ECUDA, std::string("generic counters: ") + cudaGetErrorString(e));
   if (nitems <= 0) return SQB200_OK;
-  int rc = set_smem();
-  if (rc) return rc;
   GenArgs a = make_args(g);
   a.b = b;
   k_jk_gen<<<nitems, 32 * kGenWarps, kGenSmem, st>>>(a, d_items);

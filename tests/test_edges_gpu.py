@@ -1,8 +1,11 @@
 """Edge cases of the J/K build against the oracle port: the smallest basis (one s function),
 a zero density, a density with a single non-zero pair, a cutoff no quartet passes, an sp-shell
-basis with one f shell added (the generic path with L-shell kets), and the inputs the library
-must refuse (a g function, a contraction longer than the reference's MAXCONTRACT of 32)."""
+basis with one f shell added (the generic path with L-shell kets), every screen off against the
+reference's unscreened quadruple loop, and the inputs the library must refuse (a g function, a
+contraction longer than the reference's MAXCONTRACT of 32)."""
 import ctypes
+import os
+import tempfile
 
 import numpy as np
 import pytest
@@ -111,3 +114,37 @@ def test_g_function_and_long_contraction_refused():
     assert rc == -2 and b"l+m+n = 4" in msg
     rc, msg = _create(_basis([(33, (0, 0, 0), (0.0, 0.0, 0.0), list(np.geomspace(0.1, 100.0, 33)), [0.1] * 33)]))
     assert rc == -2 and b"contraction" in msg
+
+
+def _ref_inputs(d, g):
+    """The molecule and the basis text (written by the package) for a run of the reference."""
+    sqb = load_sqb200()
+    xyz = os.path.join(d, "m.xyz")
+    with open(xyz, "w") as f:
+        f.write(sqb.molecules.xyz_text([(int(a[0]), a[1], a[2], a[3]) for a in g["atoms"]]))
+    bas = os.path.join(d, "b.txt")
+    with open(bas, "w") as f:
+        f.write(sqb.basis.gamess_text(str(g["basis"]), [int(a[0]) for a in g["atoms"]]))
+    return xyz, bas
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not port.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("case", ["water_321g", "oh_321g_uhf"])
+def test_unscreened_build_matches_reference_quadruple_loop(case):
+    """With every screen off (cutoff 0, no density screen) the build equals the reference's
+    unscreened loop over all function quartets, GTO_JK_Matrix_NoSymm, to 1e-10: the symmetric
+    shell-quartet digestion, the degeneracy factors and the J/K signs, with nothing skipped but
+    primitive quartets below the 1e-15 prefactor (which that loop keeps)."""
+    sqb = load_sqb200()
+    g = golden(case)
+    restricted = bool(g["restricted"])
+    PB = None if restricted else g["PB"]
+    with tempfile.TemporaryDirectory() as d:
+        xyz, bas = _ref_inputs(d, g)
+        GA, GB = port.ref_nosymm(xyz, bas, g["PA"], PB, cutoff=0.0)
+    eng = sqb.JKEngine(golden_basis(g), schwarz=g["schwarz"])
+    JT, KA, KB = eng.build(g["PA"], PB, restricted=restricted, scf_cutoff=0.0, dscreen_rmax=float("inf"))
+    eng.close()
+    assert np.abs(JT + KA - GA).max() <= TOL
+    assert np.abs(JT + KB - GB).max() <= TOL
