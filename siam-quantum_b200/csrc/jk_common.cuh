@@ -4,7 +4,8 @@
 // src/fgamma.c:172-206).  Written from the mathematics, not from any library:
 //   T <  BOYS_TMAX : the top order F_M(T) by a 9-term Taylor expansion about the nearest grid
 //                    point T0 (spacing BOYS_H), F_M(T0+d) = sum_k F_{M+k}(T0) (-d)^k / k!,
-//                    then the stable downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1).
+//                    then the stable downward recursion F_m = (2T F_{m+1} + e^-T)/(2m+1), with
+//                    e^-T = e^-T0 e^-d from a tabulated e^-T0 and the Taylor series of e^-d.
 //   T >= BOYS_TMAX : F_0 = sqrt(pi/T)/2 (the erfc tail is below 1e-17 relative there) and the
 //                    stable upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T).
 // The grid values are computed on the host in extended precision (jk_engine.cu).
@@ -140,7 +141,13 @@ __device__ __forceinline__ void boys(double T, const double* __restrict__ tab, d
     for (int k = BOYS_NTAY - 2; k >= 0; --k) s = fma(s, -d * (1.0 / (double)(k + 1)), row[k]);
     F[M] = s;
     if (M > 0) {
-      const double e = exp(-T);
+      // e^-T = e^-T0 e^-d: the grid value (stored after the table's rows) times the Taylor
+      // series of e^-d through d^9/9! (|d| <= 0.05: the next term is below 3e-20)
+      const double e0 = __ldg(tab + BOYS_NGRID * BOYS_NCOL + g);
+      double ed = 1.0;
+#pragma unroll
+      for (int k = 9; k >= 1; --k) ed = fma(ed, -d * (1.0 / (double)k), 1.0);
+      const double e = e0 * ed;
       const double t2 = T + T;
 #pragma unroll
       for (int m = M - 1; m >= 0; --m) F[m] = fma(t2, F[m + 1], e) * (1.0 / (2 * m + 1));

@@ -144,7 +144,12 @@ std::vector<double> boys_table(int ncol) {
 
 namespace {
 
-std::vector<double> make_boys_table() { return sqb::boys_table(BOYS_NCOL); }
+// the class kernels' table: BOYS_NGRID rows of BOYS_NCOL orders, then e^-T0 per grid point
+std::vector<double> make_boys_table() {
+  std::vector<double> t = sqb::boys_table(BOYS_NCOL);
+  for (int g = 0; g < BOYS_NGRID; ++g) t.push_back((double)expl(-(long double)g * (long double)BOYS_H));
+  return t;
+}
 
 // ---------------------------------------------------------------- shells
 
