@@ -592,7 +592,7 @@ def run_reference_split(args, atoms, bname, PA, desc, procs, sqb):
 # is profiles/<kernel>_<workload>.md.  Kernels without a capture report null.
 TRAFFIC = {("benzene", "jk_DL_LL_R"): 912384, ("benzene", "jk_DL_LL_R_w"): 845312,
            ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768, ("c60", "jk_LL_LL_R_w"): 20667648,
-           ("water-qzp", "k_jk_gen"): 1665536}
+           ("water-qzp", "k_jk_gen"): 1336320}
 
 
 def max_over_ranks(dist, t_local, device):
