@@ -590,8 +590,8 @@ def run_reference_split(args, atoms, bname, PA, desc, procs, sqb):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the dominant class
 # kernel, from one `ncu --set full` capture of the same workload; the summary with its command
 # is profiles/<kernel>_<workload>.md.  Kernels without a capture report null.
-TRAFFIC = {("benzene", "jk_DL_LL_R"): 912384, ("benzene", "jk_DL_LL_R_w"): 845312,
-           ("benzene", "jk_DL_LL_R_s"): 1180672, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768, ("c60", "jk_LL_LL_R_w"): 20667648,
+TRAFFIC = {("benzene", "jk_DL_LL_R"): 970752, ("benzene", "jk_DL_LL_R_w"): 890112,
+           ("benzene", "jk_DL_LL_R_s"): 1268992, ("c60-synthetic", "jk_LL_LL_R_w"): 18592768, ("c60", "jk_LL_LL_R_w"): 20667648,
            ("water-qzp", "k_jk_gen"): 1336320}
 
 
