@@ -973,14 +973,12 @@ void sort_heavy_first(std::vector<sqb::WorkItem>& v, size_t first, F nprims) {
 // A class whose FP32 work items would number fewer than this runs all its quartets in FP64: a
 // second launch of a few hundred CTAs costs more than its FP32 arithmetic saves, and splitting
 // the ket ranges at the FP32 threshold leaves the FP64 items shorter (SQB200_F32_MIN_ITEMS,
-// default 600; measured on B200: benzene/6-31G* at tau 1e-5 0.896 ms with no minimum, 0.758
-// with 600, 0.744 with 1200, against 0.748 in FP64; C60 51.05 ms either way).
+// default 2400, read whenever a work list is made; measured on B200: benzene/6-31G* at tau 1e-5
+// 0.729 ms with 600, 0.725 with 1200, 0.716 with 2400, against 0.713-0.720 in FP64; C60/6-31G
+// 50.5 ms with each, against 63.1 in FP64).
 size_t f32_min_items() {
-  static const size_t n = [] {
-    const char* e = getenv("SQB200_F32_MIN_ITEMS");
-    return e ? (size_t)std::max(0L, atol(e)) : (size_t)600;
-  }();
-  return n;
+  const char* e = getenv("SQB200_F32_MIN_ITEMS");
+  return e ? (size_t)std::max(0L, atol(e)) : (size_t)2400;
 }
 
 // True when a class's FP32 items are too few to launch: the class then runs all its quartets

@@ -31,7 +31,10 @@ def test_tau_zero_is_plain_fp64():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("case", ["benzene_631gs", "oh_321g_uhf"])
-def test_mixed_error_shrinks_with_tau(case):
+def test_mixed_error_shrinks_with_tau(case, monkeypatch):
+    # every class with quartets below tau takes its FP32 form, however few its FP32 work items
+    # (by default a class with few of them stays in FP64)
+    monkeypatch.setenv("SQB200_F32_MIN_ITEMS", "0")
     g = golden(case)
     restricted = bool(g["restricted"])
     eng = _engine(g)
