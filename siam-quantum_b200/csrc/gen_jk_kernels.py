@@ -91,6 +91,21 @@ if USE_WS:
     raise SystemExit("SQB_WS: the warp-specialised form reads primitive records field-contiguously; "
                      "the pair arrays now store each record's fields kstride apart")   # also emit warp-specialised multi-pass kernels (measured slower on B200; opt-in)
 CTA = 128
+# Register caps (__maxnreg__) for kernels where a cap measured faster on B200: with fewer
+# registers per thread more 64-thread CTAs share an SM, which pays where the spills it adds stay
+# small.  C60/6-31G build, restricted forms (ms per build, uncapped -> capped): LL|LS wide
+# 17.20 -> 16.19 at 128 registers (16.48 at 168, 17.70 at 144, 255 uncapped); LS|LS swapped
+# 3.61 -> 3.12 at 128 (144 uncapped, no spills either way; 3.22 at 112).  LL|LL wide stays
+# uncapped (40.4 ms; 42.3 at 168, 47.2 at 200).  The unrestricted forms are not capped.
+REG_CAP = {"jk_LL_LS_R_w": 128, "jk_LS_LS_R_s": 128}
+
+
+def kernel_qualifiers(name, bounds):
+    """The launch qualifier of kernel `name`: its register cap if it has one, else
+    __launch_bounds__(bounds)."""
+    if name in REG_CAP:
+        return "__maxnreg__(%d)" % REG_CAP[name]
+    return "__launch_bounds__(%s)" % bounds
 
 
 def pair_funcs(pc):
@@ -283,8 +298,8 @@ def gen_class(bra, ket, spin, prec="D", state_max=None, suffix="", smem_o=False,
                     "  sboys[x] = a.boys_tab%s[(x / %d) * BOYS_NCOL + %d + x %% %d];" % ("_f" if F32 else "", bnc, bc0, bnc),
                     "__syncthreads();"]
     minb = MIN_BLOCKS_NARROW if (MIN_BLOCKS_NARROW and suffix == "" and not F32) else MIN_BLOCKS
-    out.append('extern "C" __global__ void __launch_bounds__(%s)' % (
-        "%d, %d" % (CTA, minb) if minb else "%d" % CTA))
+    out.append('extern "C" __global__ void %s' % kernel_qualifiers(
+        name, "%d, %d" % (CTA, minb) if minb else "%d" % CTA))
     out.append("%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name)
     if F32:
         em("extern __shared__ float sbra_f32[];")
@@ -626,7 +641,7 @@ def gen_class_swap(bra, ket, spin, state_max):
     fl = {"prim": 0, "flush": 0, "quartet": 0, "passes": len(blocks),
           "alg_prim": alg_prim_flops(fk, Hb_all, "double", "fma"), "o_dbl": per * ncd if SO else 0}
     em = Emitter()
-    out = ['extern "C" __global__ void __launch_bounds__(%d)' % CTA,
+    out = ['extern "C" __global__ void %s' % kernel_qualifiers(name, "%d" % CTA),
            "%s(const sqb::JKArgs a, const sqb::WorkItem* __restrict__ items) {" % name]
     em("extern __shared__ double sbra[];")
     if SO:
