@@ -642,10 +642,16 @@ def run_ours(args, sqb):
         eng.build_device(PA.data_ptr(), PA.data_ptr(), JT.data_ptr(), KA.data_ptr(), None,
                          stream=stream.cuda_stream, **kw)
 
-    if not args.no_autotune:
-        # untimed set-up: per class, the faster of the narrow and wide tile forms on this work
+    if args.tiles_from:
+        # the forms an earlier run chose (a profiler serialises the autotuner's timed launches,
+        # so under one it would choose differently from the timed run it explains)
+        eng.set_tiles(np.loadtxt(args.tiles_from, dtype=np.int32, ndmin=1))
+    elif not args.no_autotune:
+        # untimed set-up: per class, the fastest of the narrow, wide and swapped forms on this work
         eng.autotune(PA.data_ptr(), stream=stream.cuda_stream, **kw)
     tiles = eng.tiles()
+    if args.save_tiles and rank == 0:
+        np.savetxt(args.save_tiles, tiles, fmt="%d")
 
     for _ in range(args.warmup):
         step()
@@ -741,7 +747,8 @@ def run_ours(args, sqb):
                        "quartets_per_build": st["quartets"], "prim_quartets_per_build": st["prim_quartets"],
                        "tiles": ("autotuned forms per class: %d narrow, %d wide, %d swapped" % (
                            int((tiles == 0).sum()), int((tiles == 1).sum()), int((tiles == 2).sum()))
-                                 if not args.no_autotune else "narrow")},
+                                 if not args.no_autotune else "narrow")
+                                if not args.tiles_from else "forms per class from %s" % args.tiles_from},
             "quartets_per_s": value * st["quartets"], "prim_quartets_per_s": value * st["prim_quartets"],
             "e2e": e2e, "roofline": roof, "clocks": clk,
             "gpu_launches": args.steps * st["launches"],
@@ -799,6 +806,10 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep every class on its narrow tile")
+    ap.add_argument("--save-tiles", default="", help="write the per-class forms the run used to this file")
+    ap.add_argument("--tiles-from", default="",
+                    help="J/K workloads: take the per-class forms from this file (written by --save-tiles) "
+                         "instead of autotuning")
     ap.add_argument("--fp32-below", type=float, default=0.0,
                     help="mixed precision: quartets with Schwarz product below this run in FP32")
     ap.add_argument("--persistent", action="store_true",
